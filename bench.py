@@ -1,0 +1,432 @@
+#!/usr/bin/env python
+"""Optical photons traced per second on B200: the batched FP32 engine on the
+uneven-event workload, next to the plain one-event-per-launch FP64 form and
+the CPU port of the reference algorithm.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU (launched by torchrun for N > 1); every rank transports
+its own seeded copy of the workload (weak scaling: events are independent, no
+data-path collective). A step is one pass of the transport over the batch.
+`value` times the device path with the gensteps already in HBM
+(g4b_relaunch); `e2e` times the public API with host buffers (g4b_enqueue
+with the host-to-device copy of the gensteps, g4b_complete with the ordered
+detections copied back to pinned host memory). Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Optical photons traced/s on 1 B200: batched FP32 vs plain form, same accuracy"
+UNIT = "photons/s"
+WORKLOAD_TEXT = ("50,000 e- events, energy log-uniform 0.1-20 MeV, entry uniform on the 3x3 mm face, incidence "
+                 "uniform to 30 deg, 10,000 ph/MeV scintillation (40 ns, 420+-20 nm) + Cerenkov (n=1.82); "
+                 "3x3x10 mm crystal, 0.95 specular wrapper, 0.1 mm n=1.41 grease, SiPM PDE 0.3")
+
+
+def parse_args():
+    parser = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=5)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    parser.add_argument("--events", type=int, default=50000, help="events per rank (the workload has 50,000)")
+    parser.add_argument("--plain-events", type=int, default=1000,
+                        help="events of the same workload timed in the plain FP64 form")
+    parser.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample length")
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--no-plain", action="store_true")
+    parser.add_argument("--no-e2e", action="store_true")
+    parser.add_argument("--no-autotune", action="store_true")
+    return parser.parse_args()
+
+
+def distributed():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._proc = None
+        self._thread = None
+
+    def start(self):
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device_index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self._proc = None
+            return
+        self._thread = threading.Thread(target=self._read, daemon=True)
+        self._thread.start()
+
+    def _read(self):
+        for line in self._proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+        if self._thread is not None:
+            self._thread.join(timeout=5)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        mhz = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        max_mhz = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i].lower() == "active"})
+        return {
+            "sm_mhz": statistics.median(mhz) if mhz else None,
+            "sm_max_mhz": max(max_mhz) if max_mhz else None,
+            "reasons": reasons,
+            "samples": len(self.samples),
+        }
+
+
+def measured_peaks():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return data, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def profile_inputs():
+    """Per-photon-step instruction count and DRAM traffic per photon from the
+    committed ncu summary of the batched FP32 kernel (profiles/), if present."""
+    path = ROOT / "profiles" / "roofline_inputs.json"
+    if path.exists():
+        return json.loads(path.read_text())
+    return {}
+
+
+def run_oracle_sample(batch, scene, seconds: float, seed: int):
+    """The CPU port (FP64, all host threads) on growing slices of the batch until ~`seconds` of work."""
+    from g4go_b200 import PhotonTransportConfig
+    from oracle import binding
+
+    config = PhotonTransportConfig(seed=seed, precision="fp64")
+    threads = os.cpu_count() or 1
+    total = batch.photon_count
+    begin = 0
+    chunk = 200_000
+    photons = 0
+    elapsed = 0.0
+    while elapsed < seconds and begin < total:
+        end = min(begin + chunk, total)
+        t0 = time.perf_counter()
+        binding.transport(scene, batch, config, threads=threads, photon_range=(begin, end))
+        dt = time.perf_counter() - t0
+        elapsed += dt
+        photons += end - begin
+        begin = end
+        if dt < seconds / 8:
+            chunk *= 2
+    return photons, elapsed, threads
+
+
+def bench_reference(args, world, rank):
+    """Reference arm: the CPU port of the reference's algorithm on the host cores."""
+    if rank != 0:
+        return
+    from g4go_b200 import scenes
+
+    scene = scenes.crystal_sipm_scene()
+    batch = scenes.workload("batched", event_count=min(args.events, 5000), seed=1)
+    step_seconds = max(2.0, min(10.0, 60.0 / max(args.steps + args.warmup, 1)))
+    for _ in range(args.warmup):
+        run_oracle_sample(batch, scene, step_seconds / 4, seed=7)
+    photons = 0
+    elapsed = 0.0
+    threads = os.cpu_count() or 1
+    for _ in range(args.steps):
+        p, e, threads = run_oracle_sample(batch, scene, step_seconds, seed=7)
+        photons += p
+        elapsed += e
+    value = photons / elapsed
+    sample = (f"{photons / args.steps:.3g} photons per step from the first events of the workload "
+              f"(FP64 CPU port, {threads} threads)")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * elapsed / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_TEXT, "events": args.events, "impl": "oracle port (reference CPU path "
+                   "is Geant4, not installed here)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def bench_ours(args, world, rank, local):
+    import torch
+
+    from g4go_b200 import DETECTION_DTYPE, PhotonTransportConfig, TransportHost, scenes
+    from g4go_b200 import _abi
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    scene = scenes.crystal_sipm_scene()
+    t0 = time.perf_counter()
+    batch = scenes.workload("batched", event_count=args.events, seed=1 + rank, first_event_id=rank * args.events)
+    synth_seconds = time.perf_counter() - t0
+    photons = batch.photon_count
+    emissions = batch.emissions.shape[0]
+    events = batch.event_ids.shape[0]
+
+    # Autotune the launch shape on a sample of the workload (block size x blocks/SM x queue chunk).
+    tuned = {}
+    if not args.no_autotune:
+        sample = scenes.workload("batched", event_count=min(2000, args.events), seed=1 + rank)
+        with TransportHost(PhotonTransportConfig(seed=7, device=local)) as tuner:
+            tuner.enqueue_emissions(scene, sample)
+            tuner.complete_oldest_batch(counts_only=True)
+            tuned = tuner.autotune(repeats=2)
+    config = PhotonTransportConfig(
+        seed=7, device=local, precision="fp32", launch_form="batched", use_cuda_graph=True,
+        block_size=tuned.get("block_size", 0), blocks_per_sm=tuned.get("blocks_per_sm", 0),
+        chunk_photons=tuned.get("chunk_photons", 0),
+    )
+    host = TransportHost(config)
+    stream = torch.cuda.ExternalStream(host.stream, device=torch.device("cuda", local))
+
+    # Stage the batch (host -> device once) and warm up.
+    host.enqueue_emissions(scene, batch)
+    first = host.complete_oldest_batch(counts_only=True)
+    hits_per_step = first.statistics["detected_count"]
+    bounces = first.performance["total_bounce_count"]
+    for _ in range(max(args.warmup - 1, 0)):
+        host.relaunch()
+        host.complete_oldest_batch(counts_only=True)
+
+    # Timed device path: K relaunches on the resident gensteps.
+    sampler = ClockSampler(local)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    kernel_ms = []
+    launches = 0
+    start.record(stream)
+    for _ in range(args.steps):
+        host.relaunch()
+        out = host.complete_oldest_batch(counts_only=True)
+        kernel_ms.append(out.performance["kernel_ms"])
+        launches += out.performance["kernel_launch_count"]
+        if out.statistics["detected_count"] != hits_per_step:
+            raise RuntimeError("relaunch is not deterministic")
+    stop.record(stream)
+    torch.cuda.synchronize()
+    sampler.stop()
+    elapsed_ms = start.elapsed_time(stop)
+    if world > 1:
+        t = torch.tensor([elapsed_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    ms_per_step = elapsed_ms / args.steps
+    value = photons * world / (ms_per_step / 1000.0)
+
+    # End to end through the public API: host gensteps in, ordered detections back to pinned memory.
+    e2e = None
+    if not args.no_e2e:
+        pinned = C_pinned(_abi, max(hits_per_step, 1) * DETECTION_DTYPE.itemsize)
+        detections = np.frombuffer(pinned.buffer, dtype=DETECTION_DTYPE)
+        host_emissions = C_pinned(_abi, emissions * 128)
+        staged = np.frombuffer(host_emissions.buffer, dtype=_abi.EMISSION_DTYPE)
+        staged[:] = batch.emissions
+        from g4go_b200 import PhotonTransportBatch
+
+        pinned_batch = PhotonTransportBatch(staged, batch.event_ids, batch.emission_event_indices)
+        host.enqueue_emissions(scene, pinned_batch)
+        host.complete_oldest_batch(detections_out=detections)
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        e2e_start = torch.cuda.Event(enable_timing=True)
+        e2e_stop = torch.cuda.Event(enable_timing=True)
+        e2e_steps = max(1, min(args.steps, 3))
+        e2e_start.record(stream)
+        h2d = d2h = 0
+        for _ in range(e2e_steps):
+            host.enqueue_emissions(scene, pinned_batch)
+            out = host.complete_oldest_batch(detections_out=detections)
+            h2d = out.performance["host_to_device_bytes"]
+            d2h = out.performance["device_hits_to_host_bytes"] + out.performance["device_metadata_to_host_bytes"]
+        e2e_stop.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = e2e_start.elapsed_time(e2e_stop) / e2e_steps
+        if world > 1:
+            t = torch.tensor([e2e_ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e = {"value": photons * world / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms}
+        del detections, staged, pinned_batch
+        pinned.free()
+        host_emissions.free()
+
+    # The plain form: one event per launch, one thread per photon, FP64, on the first events of the workload.
+    plain = None
+    if not args.no_plain and rank == 0:
+        plain_batch = scenes.workload("batched", event_count=min(args.plain_events, args.events), seed=1 + rank)
+        with TransportHost(PhotonTransportConfig(seed=7, device=local, precision="fp64", launch_form="plain")) as ph:
+            ph.enqueue_emissions(scene, plain_batch)
+            ph.complete_oldest_batch(counts_only=True)
+            pstream = torch.cuda.ExternalStream(ph.stream, device=torch.device("cuda", local))
+            ps = torch.cuda.Event(enable_timing=True)
+            pe = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            ps.record(pstream)
+            ph.relaunch()
+            pout = ph.complete_oldest_batch(counts_only=True)
+            pe.record(pstream)
+            torch.cuda.synchronize()
+            plain_ms = ps.elapsed_time(pe)
+        plain = {"value": plain_batch.photon_count / (plain_ms / 1000.0), "unit": UNIT,
+                 "events": int(plain_batch.event_ids.shape[0]), "photons": int(plain_batch.photon_count),
+                 "ms": plain_ms, "launches": int(pout.performance["kernel_launch_count"])}
+
+    clocks = sampler.summary()
+    host.close()
+
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        cpu_photons, cpu_seconds, cores = run_oracle_sample(batch, scene, args.cpu_seconds, seed=7)
+        cpu = {"value": cpu_photons / cpu_seconds, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"first {cpu_photons} photons of the workload's gensteps, FP64 CPU port of the "
+                         f"reference algorithm, {cores} threads, {cpu_seconds:.1f} s"}
+
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+
+    peaks, peak_kind = measured_peaks()
+    kernel_mean_ms = sum(kernel_ms) / len(kernel_ms)
+    algorithmic_bytes = emissions * (128 + 4 + 4) + 4 + hits_per_step * 48 + events * 64 + 64
+    achieved_gbs = algorithmic_bytes / (kernel_mean_ms / 1000.0) / 1e9
+    prof = profile_inputs()
+    traffic = None
+    if "dram_bytes_per_photon" in prof:
+        traffic = prof["dram_bytes_per_photon"] * photons
+    roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved_gbs / peaks["hbm_gbs"], "traffic": traffic,
+                "peak_kind": f"{peak_kind} (STREAM copy)",
+                "note": "the transport is instruction-issue bound; see issue_roofline"}
+    steps_per_s = bounces / (kernel_mean_ms / 1000.0)
+    issue = None
+    clock_mhz = clocks.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    if "lane_ops_per_step" in prof:
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        peak_ops = sms * 4 * 32 * clock_mhz * 1e6
+        achieved_ops = steps_per_s * prof["lane_ops_per_step"]
+        issue = {"achieved": achieved_ops, "peak": peak_ops, "unit": "lane-instructions/s",
+                 "frac": achieved_ops / peak_ops, "lane_ops_per_step": prof["lane_ops_per_step"],
+                 "sm_mhz": clock_mhz, "source": prof.get("source")}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {
+            "workload": WORKLOAD_TEXT, "events_per_gpu": events, "gensteps_per_gpu": emissions,
+            "photons_per_gpu": photons, "form": "batched persistent kernel, device work queue, CUDA graph",
+            "precision": "fp32 transport, fp64 global time and TIR test",
+            "launch": {"block_size": host.config.block_size or tuned.get("block_size"),
+                       "blocks_per_sm": tuned.get("blocks_per_sm"), "chunk_photons": tuned.get("chunk_photons"),
+                       "autotune_best_ms_on_sample": tuned.get("best_ms")},
+            "l2": "inputs larger than L2: %.0f MB of gensteps per step" % (emissions * 128 / 1e6),
+            "synthesis_seconds": synth_seconds,
+        },
+        "e2e": e2e,
+        "roofline": roofline,
+        "issue_roofline": issue,
+        "photon_steps_per_s": steps_per_s * world,
+        "mean_steps_per_photon": bounces / photons,
+        "detected_fraction": hits_per_step / photons,
+        "kernel_ms": kernel_mean_ms,
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "plain_fp64": plain,
+        "batched_over_plain": (value / world / plain["value"]) if plain else None,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+class C_pinned:
+    """Page-locked host buffer from the engine (g4b_host_alloc)."""
+
+    def __init__(self, abi, nbytes: int):
+        import ctypes as C
+
+        self._abi = abi
+        self._lib = abi.load()
+        self.pointer = C.c_void_p()
+        status = self._lib.g4b_host_alloc(nbytes, C.byref(self.pointer))
+        if status != 0:
+            raise RuntimeError("g4b_host_alloc failed")
+        self.buffer = (C.c_ubyte * nbytes).from_address(self.pointer.value)
+
+    def free(self):
+        if self.pointer:
+            self.buffer = None
+            self._lib.g4b_host_free(self.pointer)
+            self.pointer = None
+
+
+def main():
+    args = parse_args()
+    world, rank, local = distributed()
+    if args.impl == "reference":
+        bench_reference(args, world, rank)
+        return
+    bench_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

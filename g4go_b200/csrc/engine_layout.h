@@ -1,0 +1,155 @@
+// engine_layout.h - data layout shared by the engine's host code and kernels.
+//
+// The analytic scene is packed on the host into one blob that every CTA
+// copies into shared memory at launch: boxes, per-volume metadata, a dense
+// (from, to) -> surface table, materials, surfaces, and one pool of property
+// floats. Launch parameters travel by value in the kernel's constant bank.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+namespace g4b {
+
+constexpr std::uint32_t kInvalidID = 0xffffffffU;
+constexpr std::uint32_t kMaxVolumes = 64;
+constexpr std::uint32_t kMaxMaterials = 16;
+constexpr std::uint32_t kMaxSurfaces = 16;
+constexpr std::uint32_t kMaxPoolFloats = 6144;
+constexpr std::uint8_t kNoSurface = 0xff;
+constexpr std::uint8_t kNoVolume = 0xff;
+
+// A property table in the pool: energies at [offset, offset + count), values
+// at [offset + count, offset + 2 * count). count == 0: absent.
+struct PackedProperty {
+    std::uint16_t offset;
+    std::uint16_t count;
+    std::uint16_t constant;  // PropertyTable::Constant (src/optical/Scene.cpp:184-188)
+    std::uint16_t reserved;
+};
+
+struct PackedMaterial {
+    PackedProperty rindex;
+    PackedProperty groupVelocity;
+    PackedProperty absLength;
+    PackedProperty rayleighLength;
+    PackedProperty spectrum[3];  // energies + normalised CDF
+    float rindexMax;
+    std::uint32_t reserved;
+};
+
+struct PackedSurface {
+    std::uint8_t type;
+    std::uint8_t model;
+    std::uint8_t finish;
+    std::uint8_t reserved0;
+    float modelValue;
+    PackedProperty reflectivity;
+    PackedProperty efficiency;
+    PackedProperty transmittance;
+    PackedProperty rindex;
+    PackedProperty specularLobe;
+    PackedProperty specularSpike;
+    PackedProperty backscatter;
+    PackedProperty roughness;
+};
+
+// Box as two float4 (lo.xyz, hi.xyz; w unused) for 16-byte shared loads.
+struct PackedBox {
+    float lo[4];
+    float hi[4];
+};
+
+struct PackedVolume {
+    std::uint8_t parent;          // dense index or kNoVolume
+    std::uint8_t material;
+    std::uint8_t coincidentFaces; // bit f: face f = 2*axis + side touches another volume
+    std::uint8_t mayCoincide;     // Volume::mayHaveCoincidentBoundary
+    std::uint32_t sensorID;       // kInvalidID if not a sensor
+};
+
+struct PackedScene {
+    std::uint32_t volumeCount;
+    std::uint32_t materialCount;
+    std::uint32_t surfaceCount;
+    std::uint32_t poolFloats;
+    std::uint32_t world;
+    std::uint32_t hasRayleigh;
+    std::uint32_t reserved[2];
+    PackedBox boxes[kMaxVolumes];
+    PackedVolume volumes[kMaxVolumes];
+    PackedMaterial materials[kMaxMaterials];
+    PackedSurface surfaces[kMaxSurfaces];
+    std::uint8_t surfaceTable[kMaxVolumes * kMaxVolumes];  // FindSurfaceID(from, to) or kNoSurface
+    // followed by poolFloats floats
+};
+
+static_assert(sizeof(PackedScene) % 16 == 0, "scene blob must stay 16-byte aligned");
+
+// Per-event counters (DeviceEventTransportStats, OptiXDeviceData.cuh:159-167),
+// padded to 64 bytes.
+struct EventCounters {
+    unsigned long long detected;
+    unsigned long long absorbed;
+    unsigned long long escaped;
+    unsigned long long truncated;
+    unsigned long long maxBounce;
+    unsigned long long invalid;
+    unsigned long long zeroStep;
+    unsigned long long reserved;
+};
+
+// Batch-wide counters that have no per-event breakdown, plus queue state.
+struct RunCounters {
+    unsigned long long totalBounces;
+    unsigned long long coincidentTraces;
+    unsigned long long coincidentHits;
+    unsigned long long hitCount;
+    unsigned int workTicket;
+    unsigned int reserved0;
+    unsigned long long reserved[3];
+};
+
+// Compacted hits, structure of arrays, `capacity` rows each.
+struct HitColumns {
+    float* positionX;
+    float* positionY;
+    float* positionZ;
+    float* time;
+    float* directionX;
+    float* directionY;
+    float* directionZ;
+    float* energy;
+    std::uint32_t* eventID;
+    std::uint32_t* photonID;
+    std::uint32_t* sensorID;
+    std::uint32_t* slot;  // flattened photon index: restores the reference's order on the host
+    unsigned long long capacity;
+};
+
+struct LaunchParams {
+    const float4* emissions;               // [emissionCount] 128-byte gensteps as 8 float4 each
+    const std::uint32_t* emissionOffsets;  // [emissionCount + 1] exclusive prefix of photon counts
+    const std::uint32_t* emissionEventIndices;
+    const std::uint32_t* slotBase;         // optional [emissionCount]: flattened slot of each emission's first photon
+                                           // when the launch order differs from the batch order (plain form)
+    const PackedScene* scene;              // device copy of the blob
+    std::uint32_t sceneBytes;
+    std::uint32_t emissionCount;
+    std::uint32_t eventCount;
+    std::uint32_t photonBegin;             // first flattened photon of this launch
+    std::uint32_t photonEnd;               // one past the last
+    std::uint32_t emissionBegin;           // plain form: first emission of the event
+    std::uint32_t emissionEnd;
+    std::uint32_t chunk;                   // batched form: photons per queue take
+    unsigned long long seed;
+    std::uint32_t maxBounce;
+    float epsilon;
+    EventCounters* events;
+    RunCounters* run;
+    HitColumns hits;
+    std::uint32_t* photonFate;             // optional [photons]
+    double* photonTime;                    // optional [photons]
+};
+
+}  // namespace g4b

@@ -1,0 +1,46 @@
+// kernels.h - host-side entry points into the engine's CUDA kernels.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "engine_layout.h"
+
+namespace g4b {
+
+enum KernelPrecision : int { kFP32 = 0, kFP64 = 1 };
+enum KernelForm : int { kBatched = 0, kPlain = 1 };
+
+// The transport kernel for (precision, form), as a function pointer usable in
+// cudaLaunchKernel and in graph kernel nodes.
+const void* TransportKernel(int precision, int form);
+const void* ZeroCountersKernel();
+
+// Raises the dynamic shared-memory limit of every transport kernel.
+cudaError_t ConfigureTransportKernels(std::size_t sharedBytes);
+
+cudaError_t TransportOccupancy(int precision, int form, int blockSize, std::size_t sharedBytes, int* blocksPerSM);
+
+cudaError_t LaunchZeroCounters(EventCounters* events, std::uint32_t eventCount, RunCounters* run, cudaStream_t stream);
+
+cudaError_t LaunchTransport(const LaunchParams& params, int precision, int form, unsigned grid, unsigned block,
+                            std::size_t sharedBytes, cudaStream_t stream);
+
+// Ordered compaction: orders `count` hits by their flattened-photon slot
+// (the order cub::DeviceSelect::Flagged gives the reference,
+// src/optical/optix/OptiXHitCompaction.cu:23-30) and writes 48-byte
+// detection records. bitmap: ceil(photons/32) words; prefix: one word per
+// bitmap word; blockSums: ceil(words/1024) + 1 words.
+cudaError_t LaunchOrderHits(const HitColumns& hits, unsigned long long count, std::uint32_t photonCount,
+                            std::uint32_t* bitmap, std::uint32_t* prefix, std::uint32_t* blockSums,
+                            void* detectionsOut, bool ordered, cudaStream_t stream);
+
+cudaError_t LaunchEvalFresnel(int precision, std::uint32_t n, const double* in, double* out, cudaStream_t stream);
+cudaError_t LaunchEvalLambertian(int precision, std::uint32_t n, const double* in, double* out, cudaStream_t stream);
+cudaError_t LaunchEvalMath(std::uint32_t kind, std::uint32_t n, const float* in, float* out, cudaStream_t stream);
+cudaError_t LaunchEvalUniform(std::uint32_t n, unsigned long long seed, const unsigned long long* keys,
+                              const std::uint32_t* counters, float* out, cudaStream_t stream);
+
+}  // namespace g4b

@@ -1,0 +1,664 @@
+// transport_kernels.cu - the engine's CUDA kernels for sm_100a.
+//
+// TransportBatched: one persistent launch per batch. Every warp pulls chunks
+// of flattened photon indices from a device work queue (one atomic ticket per
+// chunk) and refills each lane as soon as its photon ends, so warps stay full
+// while histories of a few to thousands of bounces finish at different
+// times. Gensteps are read as 8 x 16-byte loads; the scene lives in shared
+// memory; detections are compacted with one atomic per warp into a
+// structure-of-arrays hit buffer; event counters accumulate per lane and are
+// flushed once per event change.
+//
+// TransportPlain: one thread per photon over one event's photons, the launch
+// layout of the reference's __raygen__rg (OptiXTransportDevice.cu:660-941).
+//
+// Both share the same generation and bounce code (g4b_device.cuh).
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "engine_layout.h"
+#include "g4b_device.cuh"
+#include "kernels.h"
+
+namespace g4b {
+
+using namespace dev;
+
+namespace {
+
+constexpr unsigned kFullMask = 0xffffffffU;
+
+extern __shared__ __align__(16) unsigned char gShared[];
+
+__device__ __forceinline__ void LoadScene(const LaunchParams& p) {
+    const uint4* source{reinterpret_cast<const uint4*>(p.scene)};
+    uint4* destination{reinterpret_cast<uint4*>(gShared)};
+    const std::uint32_t words{p.sceneBytes / 16U};
+    for (std::uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
+        destination[i] = source[i];
+    }
+    __syncthreads();
+}
+
+// Event counters of the event a lane is currently working on; flushed with
+// global atomics when the lane moves to another event and at the end.
+struct LaneCounters {
+    std::uint32_t eventIndex;
+    std::uint32_t detected, absorbed, escaped, truncated, invalid, zeroStep, maxBounce;
+
+    __device__ __forceinline__ void Reset() {
+        detected = absorbed = escaped = truncated = invalid = zeroStep = maxBounce = 0U;
+    }
+    __device__ __forceinline__ void Flush(EventCounters* events) {
+        if (eventIndex == kInvalidID) {
+            return;
+        }
+        EventCounters* e{events + eventIndex};
+        if (detected != 0U) atomicAdd(&e->detected, static_cast<unsigned long long>(detected));
+        if (absorbed != 0U) atomicAdd(&e->absorbed, static_cast<unsigned long long>(absorbed));
+        if (escaped != 0U) atomicAdd(&e->escaped, static_cast<unsigned long long>(escaped));
+        if (truncated != 0U) atomicAdd(&e->truncated, static_cast<unsigned long long>(truncated));
+        if (invalid != 0U) atomicAdd(&e->invalid, static_cast<unsigned long long>(invalid));
+        if (zeroStep != 0U) atomicAdd(&e->zeroStep, static_cast<unsigned long long>(zeroStep));
+        if (maxBounce != 0U) atomicMax(&e->maxBounce, static_cast<unsigned long long>(maxBounce));
+        Reset();
+    }
+    __device__ __forceinline__ void Switch(std::uint32_t newEvent, EventCounters* events) {
+        if (newEvent != eventIndex) {
+            Flush(events);
+            eventIndex = newEvent;
+        }
+    }
+    __device__ __forceinline__ void Finish(std::uint32_t result, std::uint32_t bounces) {
+        switch (result) {
+        case kDetected: ++detected; break;
+        case kAbsorbed: ++absorbed; break;
+        case kEscaped: ++escaped; break;
+        case kTruncated: ++truncated; break;
+        default: ++invalid; break;
+        }
+        maxBounce = max(maxBounce, bounces);
+    }
+};
+
+// Largest emission e in [begin, end) with offsets[e] <= slot (FindEmissionIndex, :304-320).
+__device__ __forceinline__ std::uint32_t FindEmission(const std::uint32_t* __restrict__ offsets, std::uint32_t begin,
+                                                      std::uint32_t end, std::uint32_t slot) {
+    std::uint32_t lo{begin};
+    std::uint32_t hi{end};
+    while (hi - lo > 1U) {
+        const std::uint32_t mid{(lo + hi) >> 1U};
+        if (__ldg(offsets + mid) <= slot) {
+            lo = mid;
+        } else {
+            hi = mid;
+        }
+    }
+    return lo;
+}
+
+// Warp-aggregated hit write: one atomic per warp reserves rows for every lane
+// that detected in this iteration; lanes then write their columns at
+// consecutive rows (coalesced). Must be reached by all 32 lanes.
+template<class R>
+__device__ __forceinline__ void WriteHits(bool write, const Photon<R>& photon, std::uint32_t sensorID,
+                                          const LaunchParams& p, unsigned lane) {
+    const unsigned mask{__ballot_sync(kFullMask, write)};
+    if (mask == 0U) {
+        return;
+    }
+    const int leader{__ffs(static_cast<int>(mask)) - 1};
+    unsigned long long base{};
+    if (static_cast<int>(lane) == leader) {
+        base = atomicAdd(&p.run->hitCount, static_cast<unsigned long long>(__popc(mask)));
+    }
+    base = __shfl_sync(kFullMask, base, leader);
+    if (write) {
+        const unsigned long long row{base + static_cast<unsigned>(__popc(mask & ((1U << lane) - 1U)))};
+        if (row < p.hits.capacity) {
+            p.hits.positionX[row] = static_cast<float>(photon.position.x);
+            p.hits.positionY[row] = static_cast<float>(photon.position.y);
+            p.hits.positionZ[row] = static_cast<float>(photon.position.z);
+            p.hits.time[row] = static_cast<float>(photon.time);
+            p.hits.directionX[row] = static_cast<float>(photon.direction.x);
+            p.hits.directionY[row] = static_cast<float>(photon.direction.y);
+            p.hits.directionZ[row] = static_cast<float>(photon.direction.z);
+            p.hits.energy[row] = static_cast<float>(photon.energy);
+            p.hits.eventID[row] = photon.eventID;
+            p.hits.photonID[row] = photon.photonID;
+            p.hits.sensorID[row] = sensorID;
+            p.hits.slot[row] = photon.slot;
+        }
+    }
+}
+
+__device__ __forceinline__ void FlushRunCounters(const LaunchParams& p, unsigned long long bounces,
+                                                 std::uint32_t coincidentTraces, std::uint32_t coincidentHits,
+                                                 unsigned lane) {
+#pragma unroll
+    for (int offset = 16; offset > 0; offset >>= 1) {
+        bounces += __shfl_down_sync(kFullMask, bounces, offset);
+    }
+    const unsigned traces{__reduce_add_sync(kFullMask, coincidentTraces)};
+    const unsigned hits{__reduce_add_sync(kFullMask, coincidentHits)};
+    if (lane == 0U) {
+        if (bounces != 0ULL) atomicAdd(&p.run->totalBounces, bounces);
+        if (traces != 0U) atomicAdd(&p.run->coincidentTraces, static_cast<unsigned long long>(traces));
+        if (hits != 0U) atomicAdd(&p.run->coincidentHits, static_cast<unsigned long long>(hits));
+    }
+}
+
+// Turns a freshly generated photon into a live one, applying the validity
+// test and the initial normalisation of __raygen__rg (:693-703).
+template<class R>
+__device__ __forceinline__ bool StartPhoton(Photon<R>& photon) {
+    const R lengthSquared{Dot(photon.direction, photon.direction)};
+    if (!(photon.energy > R(0)) || !isfinite(photon.energy) || !(lengthSquared > R(0)) || !isfinite(lengthSquared)) {
+        return false;
+    }
+    photon.direction = NormalizeChecked(photon.direction);
+    photon.polarization = ProjectPolarization(photon.polarization, photon.direction);
+    return true;
+}
+
+__device__ __forceinline__ void RecordFate(const LaunchParams& p, std::uint32_t slot, std::uint32_t result,
+                                           std::uint32_t bounces, double time) {
+    if (p.photonFate != nullptr) {
+        p.photonFate[slot] = result | (bounces << 3U);
+    }
+    if (p.photonTime != nullptr) {
+        p.photonTime[slot] = time;
+    }
+}
+
+template<class R>
+__global__ void __launch_bounds__(256) TransportBatched(const LaunchParams p) {
+    LoadScene(p);
+    const PackedScene& scene{*reinterpret_cast<const PackedScene*>(gShared)};
+    const float* pool{PoolOf(scene)};
+    const unsigned lane{threadIdx.x & 31U};
+    const unsigned lanesBelow{(1U << lane) - 1U};
+    const R epsilon{R(p.epsilon)};
+    const std::uint32_t totalPhotons{p.photonEnd - p.photonBegin};
+
+    std::uint32_t chunkNext{0U};
+    std::uint32_t chunkEnd{0U};
+    std::uint32_t cursor{0U};
+    bool queueDone{false};
+    bool alive{false};
+    Photon<R> photon{};
+    LaneCounters counters{};
+    counters.eventIndex = kInvalidID;
+    counters.Reset();
+    unsigned long long laneBounces{0ULL};
+    std::uint32_t coincidentTraces{0U};
+    std::uint32_t coincidentHits{0U};
+
+    for (;;) {
+        // Refill: lanes without a photon take the next indices of the warp's
+        // chunk; an exhausted chunk is replaced by one atomic on the ticket.
+        unsigned need{__ballot_sync(kFullMask, !alive)};
+        while (need != 0U && !queueDone) {
+            if (chunkNext >= chunkEnd) {
+                std::uint32_t start{0U};
+                if (lane == 0U) {
+                    start = atomicAdd(&p.run->workTicket, p.chunk);
+                }
+                start = __shfl_sync(kFullMask, start, 0);
+                if (start >= totalPhotons) {
+                    queueDone = true;
+                    break;
+                }
+                chunkNext = p.photonBegin + start;
+                chunkEnd = p.photonBegin + min(start + p.chunk, totalPhotons);
+                cursor = FindEmission(p.emissionOffsets, p.emissionBegin, p.emissionEnd, chunkNext);
+            }
+            const std::uint32_t available{chunkEnd - chunkNext};
+            const std::uint32_t rank{static_cast<std::uint32_t>(__popc(need & lanesBelow))};
+            const bool take{((need >> lane) & 1U) != 0U && rank < available};
+            const std::uint32_t taken{min(static_cast<std::uint32_t>(__popc(need)), available)};
+            std::uint32_t e{cursor};
+            if (take) {
+                const std::uint32_t slot{chunkNext + rank};
+                while (__ldg(p.emissionOffsets + e + 1U) <= slot) {
+                    ++e;
+                }
+                Emission emission;
+                LoadEmission(p.emissions, e, emission);
+                const std::uint32_t local{slot - __ldg(p.emissionOffsets + e)};
+                const std::uint32_t eventIndex{__ldg(p.emissionEventIndices + e)};
+                counters.Switch(eventIndex, p.events);
+                GeneratePhoton<R>(scene, pool, emission, emission.FirstPhotonID() + local, p.seed, photon);
+                photon.eventIndex = eventIndex;
+                photon.slot = (p.slotBase != nullptr) ? __ldg(p.slotBase + e) + local : slot;
+                alive = StartPhoton(photon);
+                if (!alive) {
+                    ++counters.invalid;
+                    RecordFate(p, photon.slot, kInvalid, 0U, photon.time);
+                }
+            }
+            const unsigned takeMask{__ballot_sync(kFullMask, take)};
+            cursor = __shfl_sync(kFullMask, e, 31 - __clz(static_cast<int>(takeMask)));
+            chunkNext += taken;
+            need = __ballot_sync(kFullMask, !alive);
+        }
+        if (__ballot_sync(kFullMask, alive) == 0U) {
+            break;
+        }
+
+        std::uint32_t result{kContinue};
+        StepExtras extras{0U, 0U, 0U, 0U};
+        if (alive) {
+            result = StepPhoton<R>(scene, pool, photon, p.seed, p.maxBounce, epsilon, extras);
+        }
+        WriteHits(alive && result == kDetected, photon, extras.sensorID, p, lane);
+        if (alive) {
+            counters.zeroStep += extras.zeroSteps;
+            coincidentTraces += extras.coincidentTraces;
+            coincidentHits += extras.coincidentHits;
+            if (result != kContinue) {
+                const std::uint32_t bounces{result == kTruncated ? photon.bounce : photon.bounce + 1U};
+                counters.Finish(result, bounces);
+                laneBounces += bounces;
+                RecordFate(p, photon.slot, result, bounces, photon.time);
+                alive = false;
+            }
+        }
+    }
+    counters.Flush(p.events);
+    FlushRunCounters(p, laneBounces, coincidentTraces, coincidentHits, lane);
+}
+
+template<class R>
+__global__ void __launch_bounds__(256) TransportPlain(const LaunchParams p) {
+    LoadScene(p);
+    const PackedScene& scene{*reinterpret_cast<const PackedScene*>(gShared)};
+    const float* pool{PoolOf(scene)};
+    const unsigned lane{threadIdx.x & 31U};
+    const R epsilon{R(p.epsilon)};
+    const std::uint32_t slot{p.photonBegin + blockIdx.x * blockDim.x + threadIdx.x};
+
+    LaneCounters counters{};
+    counters.eventIndex = kInvalidID;
+    counters.Reset();
+    unsigned long long laneBounces{0ULL};
+    std::uint32_t coincidentTraces{0U};
+    std::uint32_t coincidentHits{0U};
+    Photon<R> photon{};
+    bool alive{false};
+    if (slot < p.photonEnd) {
+        const std::uint32_t e{FindEmission(p.emissionOffsets, p.emissionBegin, p.emissionEnd, slot)};
+        Emission emission;
+        LoadEmission(p.emissions, e, emission);
+        const std::uint32_t local{slot - __ldg(p.emissionOffsets + e)};
+        const std::uint32_t eventIndex{__ldg(p.emissionEventIndices + e)};
+        counters.eventIndex = eventIndex;
+        GeneratePhoton<R>(scene, pool, emission, emission.FirstPhotonID() + local, p.seed, photon);
+        photon.eventIndex = eventIndex;
+        photon.slot = (p.slotBase != nullptr) ? __ldg(p.slotBase + e) + local : slot;
+        alive = StartPhoton(photon);
+        if (!alive) {
+            ++counters.invalid;
+            RecordFate(p, photon.slot, kInvalid, 0U, photon.time);
+        }
+    }
+    while (__ballot_sync(kFullMask, alive) != 0U) {
+        std::uint32_t result{kContinue};
+        StepExtras extras{0U, 0U, 0U, 0U};
+        if (alive) {
+            result = StepPhoton<R>(scene, pool, photon, p.seed, p.maxBounce, epsilon, extras);
+        }
+        WriteHits(alive && result == kDetected, photon, extras.sensorID, p, lane);
+        if (alive) {
+            counters.zeroStep += extras.zeroSteps;
+            coincidentTraces += extras.coincidentTraces;
+            coincidentHits += extras.coincidentHits;
+            if (result != kContinue) {
+                const std::uint32_t bounces{result == kTruncated ? photon.bounce : photon.bounce + 1U};
+                counters.Finish(result, bounces);
+                laneBounces += bounces;
+                RecordFate(p, photon.slot, result, bounces, photon.time);
+                alive = false;
+            }
+        }
+    }
+    counters.Flush(p.events);
+    FlushRunCounters(p, laneBounces, coincidentTraces, coincidentHits, lane);
+}
+
+__global__ void ZeroCounters(EventCounters* events, std::uint32_t eventCount, RunCounters* run) {
+    const std::uint32_t i{blockIdx.x * blockDim.x + threadIdx.x};
+    const std::uint32_t words{eventCount * static_cast<std::uint32_t>(sizeof(EventCounters) / 16U)};
+    uint4* destination{reinterpret_cast<uint4*>(events)};
+    for (std::uint32_t w = i; w < words; w += gridDim.x * blockDim.x) {
+        destination[w] = make_uint4(0U, 0U, 0U, 0U);
+    }
+    if (i < sizeof(RunCounters) / 8U) {
+        reinterpret_cast<unsigned long long*>(run)[i] = 0ULL;
+    }
+}
+
+// --- ordered compaction (bitmap of detected slots + exclusive prefix) -----
+
+__global__ void MarkSlots(const std::uint32_t* __restrict__ slots, unsigned long long count,
+                          std::uint32_t* __restrict__ bitmap) {
+    for (unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+        const std::uint32_t slot{slots[i]};
+        atomicOr(bitmap + (slot >> 5U), 1U << (slot & 31U));
+    }
+}
+
+// Block b sums the population counts of words [1024 b, 1024 b + 1024).
+__global__ void __launch_bounds__(256) BlockPopcount(const std::uint32_t* __restrict__ bitmap, std::uint32_t words,
+                                                     std::uint32_t* __restrict__ blockSums) {
+    __shared__ std::uint32_t warpSums[8];
+    const std::uint32_t base{blockIdx.x * 1024U};
+    std::uint32_t sum{0U};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const std::uint32_t w{base + threadIdx.x * 4U + static_cast<std::uint32_t>(k)};
+        if (w < words) {
+            sum += static_cast<std::uint32_t>(__popc(bitmap[w]));
+        }
+    }
+    sum = __reduce_add_sync(kFullMask, sum);
+    if ((threadIdx.x & 31U) == 0U) {
+        warpSums[threadIdx.x >> 5U] = sum;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0U) {
+        std::uint32_t total{0U};
+        for (int w = 0; w < 8; ++w) {
+            total += warpSums[w];
+        }
+        blockSums[blockIdx.x] = total;
+    }
+}
+
+// Exclusive scan of the block sums in place, one CTA of 1024 threads.
+__global__ void __launch_bounds__(1024) ScanBlockSums(std::uint32_t* sums, std::uint32_t count) {
+    __shared__ std::uint32_t warpTotals[32];
+    __shared__ std::uint32_t carry;
+    if (threadIdx.x == 0U) {
+        carry = 0U;
+    }
+    __syncthreads();
+    const unsigned lane{threadIdx.x & 31U};
+    const unsigned warp{threadIdx.x >> 5U};
+    for (std::uint32_t base = 0; base < count; base += 1024U) {
+        const std::uint32_t i{base + threadIdx.x};
+        const std::uint32_t value{i < count ? sums[i] : 0U};
+        std::uint32_t inclusive{value};
+#pragma unroll
+        for (int offset = 1; offset < 32; offset <<= 1) {
+            const std::uint32_t other{__shfl_up_sync(kFullMask, inclusive, offset)};
+            if (lane >= static_cast<unsigned>(offset)) {
+                inclusive += other;
+            }
+        }
+        if (lane == 31U) {
+            warpTotals[warp] = inclusive;
+        }
+        __syncthreads();
+        if (warp == 0U) {
+            std::uint32_t t{warpTotals[lane]};
+#pragma unroll
+            for (int offset = 1; offset < 32; offset <<= 1) {
+                const std::uint32_t other{__shfl_up_sync(kFullMask, t, offset)};
+                if (lane >= static_cast<unsigned>(offset)) {
+                    t += other;
+                }
+            }
+            warpTotals[lane] = t;
+        }
+        __syncthreads();
+        const std::uint32_t warpPrefix{warp == 0U ? 0U : warpTotals[warp - 1U]};
+        if (i < count) {
+            sums[i] = carry + warpPrefix + inclusive - value;
+        }
+        __syncthreads();
+        if (threadIdx.x == 1023U) {
+            carry += warpPrefix + inclusive;
+        }
+        __syncthreads();
+    }
+}
+
+// prefix[w] = number of set bits in words [0, w).
+__global__ void __launch_bounds__(256) WordPrefix(const std::uint32_t* __restrict__ bitmap, std::uint32_t words,
+                                                  const std::uint32_t* __restrict__ blockSums,
+                                                  std::uint32_t* __restrict__ prefix) {
+    __shared__ std::uint32_t warpTotals[8];
+    const std::uint32_t base{blockIdx.x * 1024U + threadIdx.x * 4U};
+    std::uint32_t counts[4];
+    std::uint32_t local{0U};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const std::uint32_t w{base + static_cast<std::uint32_t>(k)};
+        counts[k] = w < words ? static_cast<std::uint32_t>(__popc(bitmap[w])) : 0U;
+        local += counts[k];
+    }
+    const unsigned lane{threadIdx.x & 31U};
+    const unsigned warp{threadIdx.x >> 5U};
+    std::uint32_t inclusive{local};
+#pragma unroll
+    for (int offset = 1; offset < 32; offset <<= 1) {
+        const std::uint32_t other{__shfl_up_sync(kFullMask, inclusive, offset)};
+        if (lane >= static_cast<unsigned>(offset)) {
+            inclusive += other;
+        }
+    }
+    if (lane == 31U) {
+        warpTotals[warp] = inclusive;
+    }
+    __syncthreads();
+    std::uint32_t warpPrefix{0U};
+    for (unsigned w = 0; w < warp; ++w) {
+        warpPrefix += warpTotals[w];
+    }
+    std::uint32_t running{blockSums[blockIdx.x] + warpPrefix + inclusive - local};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const std::uint32_t w{base + static_cast<std::uint32_t>(k)};
+        if (w < words) {
+            prefix[w] = running;
+        }
+        running += counts[k];
+    }
+}
+
+// Writes each hit as a 48-byte detection record (PhotonDetection,
+// PhotonTransport.hpp:71-81) at its rank among detected slots, or at its
+// device row when `ordered` is false.
+__global__ void ScatterDetections(const HitColumns hits, unsigned long long count,
+                                  const std::uint32_t* __restrict__ bitmap, const std::uint32_t* __restrict__ prefix,
+                                  bool ordered, float4* __restrict__ out) {
+    for (unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+        unsigned long long row{i};
+        if (ordered) {
+            const std::uint32_t slot{hits.slot[i]};
+            const std::uint32_t word{slot >> 5U};
+            const std::uint32_t below{bitmap[word] & ((1U << (slot & 31U)) - 1U)};
+            row = prefix[word] + static_cast<std::uint32_t>(__popc(below));
+        }
+        float4* record{out + row * 3ULL};
+        record[0] = make_float4(hits.positionX[i], hits.positionY[i], hits.positionZ[i], hits.time[i]);
+        record[1] = make_float4(hits.directionX[i], hits.directionY[i], hits.directionZ[i], hits.energy[i]);
+        record[2] = make_float4(__uint_as_float(hits.eventID[i]), __uint_as_float(hits.photonID[i]),
+                                __uint_as_float(hits.sensorID[i]), 0.0F);
+    }
+}
+
+// --- device evaluation of single functions ------------------------------
+
+template<class R>
+__global__ void EvalFresnel(std::uint32_t n, const double* __restrict__ in, double* __restrict__ out) {
+    const std::uint32_t i{blockIdx.x * blockDim.x + threadIdx.x};
+    if (i >= n) {
+        return;
+    }
+    const double* row{in + static_cast<std::size_t>(i) * 11U};
+    const V3<R> d{R(row[0]), R(row[1]), R(row[2])};
+    const V3<R> pol{R(row[3]), R(row[4]), R(row[5])};
+    const V3<R> nrm{R(row[6]), R(row[7]), R(row[8])};
+    const FresnelOutput<R> f{ComputeFresnel(d, pol, nrm, R(row[9]), R(row[10]))};
+    double* o{out + static_cast<std::size_t>(i) * 14U};
+    const V3<R> vs[4]{f.reflectedDirection, f.transmittedDirection, f.reflectedPolarization, f.transmittedPolarization};
+    for (int k = 0; k < 4; ++k) {
+        o[3 * k] = static_cast<double>(vs[k].x);
+        o[3 * k + 1] = static_cast<double>(vs[k].y);
+        o[3 * k + 2] = static_cast<double>(vs[k].z);
+    }
+    o[12] = static_cast<double>(f.transmittance);
+    o[13] = f.tir ? 1.0 : 0.0;
+}
+
+template<class R>
+__global__ void EvalLambertian(std::uint32_t n, const double* __restrict__ in, double* __restrict__ out) {
+    const std::uint32_t i{blockIdx.x * blockDim.x + threadIdx.x};
+    if (i >= n) {
+        return;
+    }
+    const double* row{in + static_cast<std::size_t>(i) * 5U};
+    const V3<R> v{SampleLambertian(V3<R>{R(row[0]), R(row[1]), R(row[2])}, R(row[3]), R(row[4]))};
+    out[3 * i] = static_cast<double>(v.x);
+    out[3 * i + 1] = static_cast<double>(v.y);
+    out[3 * i + 2] = static_cast<double>(v.z);
+}
+
+__global__ void EvalMath(std::uint32_t kind, std::uint32_t n, const float* __restrict__ in, float* __restrict__ out) {
+    const std::uint32_t i{blockIdx.x * blockDim.x + threadIdx.x};
+    if (i >= n) {
+        return;
+    }
+    const float x{in[i]};
+    if (kind == 0U) {
+        out[i] = LogF(x);
+    } else if (kind == 1U) {
+        out[i] = ExpF(x);
+    } else {
+        float s, c;
+        SinCosTurnF(x, &s, &c);
+        out[i] = s;
+        out[n + i] = c;
+    }
+}
+
+__global__ void EvalUniform(std::uint32_t n, unsigned long long seed, const unsigned long long* __restrict__ keys,
+                            const std::uint32_t* __restrict__ counters, float* __restrict__ out) {
+    const std::uint32_t i{blockIdx.x * blockDim.x + threadIdx.x};
+    if (i >= n) {
+        return;
+    }
+    out[i] = Uniform<float>(seed, keys[i], counters[3 * i], counters[3 * i + 1], counters[3 * i + 2]);
+}
+
+unsigned BlocksFor(unsigned long long n, unsigned block) {
+    const unsigned long long blocks{(n + block - 1ULL) / block};
+    return static_cast<unsigned>(blocks == 0ULL ? 1ULL : (blocks > 1048576ULL ? 1048576ULL : blocks));
+}
+
+}  // namespace
+
+const void* TransportKernel(int precision, int form) {
+    if (form == kPlain) {
+        return precision == kFP64 ? reinterpret_cast<const void*>(&TransportPlain<double>)
+                                  : reinterpret_cast<const void*>(&TransportPlain<float>);
+    }
+    return precision == kFP64 ? reinterpret_cast<const void*>(&TransportBatched<double>)
+                              : reinterpret_cast<const void*>(&TransportBatched<float>);
+}
+
+const void* ZeroCountersKernel() { return reinterpret_cast<const void*>(&ZeroCounters); }
+
+cudaError_t ConfigureTransportKernels(std::size_t sharedBytes) {
+    for (int precision = 0; precision < 2; ++precision) {
+        for (int form = 0; form < 2; ++form) {
+            const cudaError_t error{cudaFuncSetAttribute(TransportKernel(precision, form),
+                                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                         static_cast<int>(sharedBytes))};
+            if (error != cudaSuccess) {
+                return error;
+            }
+        }
+    }
+    return cudaSuccess;
+}
+
+cudaError_t TransportOccupancy(int precision, int form, int blockSize, std::size_t sharedBytes, int* blocksPerSM) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSM, TransportKernel(precision, form), blockSize,
+                                                         sharedBytes);
+}
+
+cudaError_t LaunchZeroCounters(EventCounters* events, std::uint32_t eventCount, RunCounters* run,
+                               cudaStream_t stream) {
+    const unsigned long long words{static_cast<unsigned long long>(eventCount) * (sizeof(EventCounters) / 16U)};
+    ZeroCounters<<<BlocksFor(words < 32ULL ? 32ULL : words, 256U), 256, 0, stream>>>(events, eventCount, run);
+    return cudaGetLastError();
+}
+
+cudaError_t LaunchTransport(const LaunchParams& params, int precision, int form, unsigned grid, unsigned block,
+                            std::size_t sharedBytes, cudaStream_t stream) {
+    void* arguments[]{const_cast<LaunchParams*>(&params)};
+    return cudaLaunchKernel(TransportKernel(precision, form), dim3(grid), dim3(block), arguments, sharedBytes,
+                            stream);
+}
+
+cudaError_t LaunchOrderHits(const HitColumns& hits, unsigned long long count, std::uint32_t photonCount,
+                            std::uint32_t* bitmap, std::uint32_t* prefix, std::uint32_t* blockSums,
+                            void* detectionsOut, bool ordered, cudaStream_t stream) {
+    if (count == 0ULL) {
+        return cudaSuccess;
+    }
+    if (ordered) {
+        const std::uint32_t words{(photonCount + 31U) / 32U};
+        const std::uint32_t blocks{(words + 1023U) / 1024U};
+        cudaError_t error{cudaMemsetAsync(bitmap, 0, static_cast<std::size_t>(words) * 4U, stream)};
+        if (error != cudaSuccess) {
+            return error;
+        }
+        MarkSlots<<<BlocksFor(count, 256U), 256, 0, stream>>>(hits.slot, count, bitmap);
+        BlockPopcount<<<blocks, 256, 0, stream>>>(bitmap, words, blockSums);
+        ScanBlockSums<<<1, 1024, 0, stream>>>(blockSums, blocks);
+        WordPrefix<<<blocks, 256, 0, stream>>>(bitmap, words, blockSums, prefix);
+    }
+    ScatterDetections<<<BlocksFor(count, 256U), 256, 0, stream>>>(hits, count, bitmap, prefix, ordered,
+                                                                  static_cast<float4*>(detectionsOut));
+    return cudaGetLastError();
+}
+
+cudaError_t LaunchEvalFresnel(int precision, std::uint32_t n, const double* in, double* out, cudaStream_t stream) {
+    if (precision == kFP64) {
+        EvalFresnel<double><<<BlocksFor(n, 128U), 128, 0, stream>>>(n, in, out);
+    } else {
+        EvalFresnel<float><<<BlocksFor(n, 128U), 128, 0, stream>>>(n, in, out);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t LaunchEvalLambertian(int precision, std::uint32_t n, const double* in, double* out,
+                                 cudaStream_t stream) {
+    if (precision == kFP64) {
+        EvalLambertian<double><<<BlocksFor(n, 128U), 128, 0, stream>>>(n, in, out);
+    } else {
+        EvalLambertian<float><<<BlocksFor(n, 128U), 128, 0, stream>>>(n, in, out);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t LaunchEvalMath(std::uint32_t kind, std::uint32_t n, const float* in, float* out, cudaStream_t stream) {
+    EvalMath<<<BlocksFor(n, 256U), 256, 0, stream>>>(kind, n, in, out);
+    return cudaGetLastError();
+}
+
+cudaError_t LaunchEvalUniform(std::uint32_t n, unsigned long long seed, const unsigned long long* keys,
+                              const std::uint32_t* counters, float* out, cudaStream_t stream) {
+    EvalUniform<<<BlocksFor(n, 256U), 256, 0, stream>>>(n, seed, keys, counters, out);
+    return cudaGetLastError();
+}
+
+}  // namespace g4b

@@ -1,0 +1,122 @@
+"""The C ABI without a GPU: the library loads, exports every declared symbol,
+its record layouts match the reference's, and it fails loudly with no device."""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+HEADERS = sorted((ROOT / "include").glob("*.h"))
+
+
+def declared_functions():
+    names = set()
+    for header in HEADERS:
+        text = header.read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for match in re.finditer(r"^[A-Za-z_][\w\s\*]*?\b(g4b_\w+)\s*\(", text, flags=re.M):
+            names.add(match.group(1))
+    return sorted(names)
+
+
+def test_every_declared_symbol_is_exported(engine_lib):
+    names = declared_functions()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(engine_lib, n)]
+    assert not missing, missing
+    from g4go_b200 import _abi
+
+    assert set(names) == set(_abi.SIGNATURES), "the ctypes binding must cover exactly the declared symbols"
+
+
+def test_record_layouts_match_the_reference(tmp_path):
+    """sizeof/offsetof from a C compiler against the ctypes and numpy views."""
+    from g4go_b200 import _abi
+
+    program = tmp_path / "layout.c"
+    program.write_text(
+        '#include <stddef.h>\n#include <stdio.h>\n#include "g4b.h"\n#include "g4b_synth.h"\n'
+        "int main(void){\n"
+        ' printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n",'
+        " sizeof(g4b_optical_emission), sizeof(g4b_photon_detection), sizeof(g4b_config), sizeof(g4b_property),"
+        " sizeof(g4b_material), sizeof(g4b_surface), sizeof(g4b_volume), sizeof(g4b_scene), sizeof(g4b_statistics),"
+        " sizeof(g4b_event_statistics), sizeof(g4b_performance), sizeof(g4b_output), sizeof(g4b_synth_params),"
+        " offsetof(g4b_optical_emission, type));\n"
+        ' printf("%zu %zu %zu %zu\\n", offsetof(g4b_optical_emission, event_id),'
+        " offsetof(g4b_optical_emission, photon_count), offsetof(g4b_photon_detection, sensor_id),"
+        " offsetof(g4b_config, hit_capacity));\n"
+        " return 0; }\n"
+    )
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", str(ROOT / "include"), str(program), "-o", str(exe)], check=True)
+    first, second = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines()
+    sizes = list(map(int, first.split()))
+    offsets = list(map(int, second.split()))
+    assert sizes[0] == 128 and sizes[1] == 48  # PhotonTransport.hpp:177-178
+    expected = [_abi.EMISSION_DTYPE.itemsize, _abi.DETECTION_DTYPE.itemsize, C.sizeof(_abi.Config),
+                C.sizeof(_abi.Property), C.sizeof(_abi.Material), C.sizeof(_abi.Surface), C.sizeof(_abi.Volume),
+                C.sizeof(_abi.Scene), C.sizeof(_abi.Statistics), C.sizeof(_abi.EventStatistics),
+                C.sizeof(_abi.Performance), C.sizeof(_abi.Output), C.sizeof(_abi.SynthParams),
+                _abi.EMISSION_DTYPE.fields["type"][1]]
+    assert sizes == expected
+    # OpticalEmission field offsets (PhotonTransport.hpp:40-69): eventID at 88, photonCount at 96.
+    assert offsets[0] == 88 == _abi.EMISSION_DTYPE.fields["event_id"][1]
+    assert offsets[1] == 96 == _abi.EMISSION_DTYPE.fields["photon_count"][1]
+    assert offsets[2] == 40 == _abi.DETECTION_DTYPE.fields["sensor_id"][1]
+    assert offsets[3] == _abi.Config.hit_capacity.offset
+
+
+def test_cpp_shim_compiles(tmp_path):
+    """The header-only C++ drop-in (OptiXTransportHost signatures over the C ABI) builds and links."""
+    source = tmp_path / "shim.cpp"
+    source.write_text('#include "g4b_transport_host.hpp"\nint main(){ return 0; }\n')
+    from g4go_b200 import _abi
+
+    library = _abi.library_path()
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-I", str(ROOT / "include"), str(source),
+                    str(library), "-o", str(tmp_path / "shim")], check=True)
+
+
+def test_engine_fails_loudly_without_a_device(engine_lib):
+    from conftest import gpu_available
+    from g4go_b200 import NoDeviceError, PhotonTransportConfig, TransportHost
+
+    if gpu_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(NoDeviceError):
+        TransportHost(PhotonTransportConfig())
+
+
+def test_config_rejects_bad_abi_version(engine_lib):
+    from g4go_b200 import _abi
+
+    config = _abi.Config()
+    config.abi_version = 999
+    handle = C.c_void_p()
+    status = engine_lib.g4b_create(C.byref(config), C.byref(handle))
+    assert status == _abi.ERR_INVALID_ARGUMENT
+    assert b"abi_version" in engine_lib.g4b_last_error(None)
+
+
+def test_synthetic_gensteps_are_seeded_and_well_formed(engine_lib):
+    from g4go_b200 import scenes
+
+    a = scenes.workload("batched", event_count=300, seed=5)
+    b = scenes.workload("batched", event_count=300, seed=5)
+    c = scenes.electron_gensteps(300, **{k: v for k, v in scenes.WORKLOADS["batched"].items() if k != "event_count"},
+                                 seed=5, threads=1)
+    assert a.emissions.tobytes() == b.emissions.tobytes() == c.emissions.tobytes()
+    assert np.all(a.emissions["event_id"] == a.event_ids[a.emission_event_indices])
+    assert set(np.unique(a.emissions["type"])) <= {1, 2}
+    # photon IDs within an event are consecutive from 0
+    for event in range(5):
+        rows = a.emissions[a.emission_event_indices == event]
+        starts = rows["first_photon_id"]
+        assert starts[0] == 0
+        assert np.all(starts[1:] == starts[:-1] + rows["photon_count"][:-1])
+    # uneven events: tens to ~1e5 photons
+    per_event = np.bincount(a.emission_event_indices, weights=a.emissions["photon_count"], minlength=300)
+    assert per_event.max() > 50 * max(per_event.min(), 1)
