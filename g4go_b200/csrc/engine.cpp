@@ -212,7 +212,22 @@ namespace {
 int Precision(const g4b_handle& h) { return h.config.precision == G4B_PRECISION_FP64 ? g4b::kFP64 : g4b::kFP32; }
 int Form(const g4b_handle& h) { return h.config.launch_form == G4B_FORM_PLAIN ? g4b::kPlain : g4b::kBatched; }
 
-std::size_t SharedBytes(const g4b_handle& h) { return (static_cast<std::size_t>(h.sceneBytes) + 15U) & ~std::size_t{15}; }
+std::size_t SceneSharedBytes(const g4b_handle& h) {
+    return (static_cast<std::size_t>(h.sceneBytes) + 15U) & ~std::size_t{15};
+}
+
+// Dynamic shared memory of a launch: the scene blob, plus one photon queue
+// per warp for the batched form.
+std::size_t SharedBytes(const g4b_handle& h, int form, std::uint32_t blockSize) {
+    std::size_t bytes{SceneSharedBytes(h)};
+    if (form == g4b::kBatched) {
+        const std::size_t queue{h.config.precision == G4B_PRECISION_FP64 ? g4b::kQueueBytesFP64 : g4b::kQueueBytesFP32};
+        bytes += queue * (blockSize / 32U);
+    }
+    return bytes;
+}
+
+std::uint32_t RoundChunk(std::uint32_t chunk) { return std::max<std::uint32_t>((chunk + 31U) / 32U * 32U, 32U); }
 
 // --- scene packing ---------------------------------------------------------
 
@@ -452,6 +467,7 @@ void BuildScene(g4b_handle& h, const g4b_scene& scene) {
     // (Geant4SceneExporter.cpp:379-487). Siblings must touch with opposite
     // outward normals; parent and child may share either side.
     constexpr double tolerance{1.0e-5};
+    std::vector<std::pair<std::uint32_t, std::uint32_t>> touching;
     for (std::uint32_t i{}; i < scene.volume_count; ++i) {
         for (std::uint32_t j{i + 1}; j < scene.volume_count; ++j) {
             const bool sameParent{parents[i] != kInvalidID && parents[i] == parents[j]};
@@ -481,11 +497,25 @@ void BuildScene(g4b_handle& h, const g4b_scene& scene) {
                             packed->volumes[j].coincidentFaces |= static_cast<std::uint8_t>(1U << (2 * axis + sideSecond));
                             packed->volumes[i].mayCoincide = 1;
                             packed->volumes[j].mayCoincide = 1;
+                            touching.emplace_back(i, j);
                         }
                     }
                 }
             }
         }
+    }
+    // Trace candidates: the volume itself and its daughters. Coincidence
+    // candidates: the volume and every volume it shares a coincident face with.
+    for (std::uint32_t i{}; i < scene.volume_count; ++i) {
+        packed->volumes[i].traceMask |= 1ULL << i;
+        packed->volumes[i].neighbourMask |= 1ULL << i;
+        if (parents[i] != kInvalidID) {
+            packed->volumes[parents[i]].traceMask |= 1ULL << i;
+        }
+    }
+    for (const auto& [i, j] : touching) {
+        packed->volumes[i].neighbourMask |= 1ULL << j;
+        packed->volumes[j].neighbourMask |= 1ULL << i;
     }
     std::memset(packed->surfaceTable, g4b::kNoSurface, sizeof(packed->surfaceTable));
     for (std::uint32_t from{}; from < scene.volume_count; ++from) {
@@ -505,7 +535,8 @@ void BuildScene(g4b_handle& h, const g4b_scene& scene) {
     }
     h.dScene.Ensure(blob.size(), "cudaMalloc scene");
     Check(cudaMemcpy(h.dScene.pointer, blob.data(), blob.size(), cudaMemcpyHostToDevice), "cudaMemcpy scene");
-    Check(g4b::ConfigureTransportKernels(blob.size()), "cudaFuncSetAttribute shared memory");
+    Check(g4b::ConfigureTransportKernels(((blob.size() + 15U) & ~std::size_t{15}) + 8U * g4b::kQueueBytesFP64),
+          "cudaFuncSetAttribute shared memory");
     h.sceneBlob = std::move(blob);
     h.sceneBytes = static_cast<std::uint32_t>(h.sceneBlob.size());
     h.volumeIndex = std::move(index);
@@ -578,7 +609,8 @@ void EnsureHitCapacity(g4b_handle& h, std::uint64_t rows) {
 unsigned BatchedGrid(g4b_handle& h) {
     if (h.blocksPerSM == 0) {
         int blocks{0};
-        Check(g4b::TransportOccupancy(Precision(h), g4b::kBatched, static_cast<int>(h.blockSize), SharedBytes(h), &blocks),
+        Check(g4b::TransportOccupancy(Precision(h), g4b::kBatched, static_cast<int>(h.blockSize),
+                                      SharedBytes(h, g4b::kBatched, h.blockSize), &blocks),
               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
         h.blocksPerSM = static_cast<std::uint32_t>(std::max(blocks, 1));
     }
@@ -617,7 +649,7 @@ void LaunchBatchedGraph(g4b_handle& h, const LaunchParams& params, unsigned grid
     transport.func = const_cast<void*>(g4b::TransportKernel(Precision(h), g4b::kBatched));
     transport.gridDim = dim3(grid);
     transport.blockDim = dim3(h.blockSize);
-    transport.sharedMemBytes = static_cast<unsigned>(SharedBytes(h));
+    transport.sharedMemBytes = static_cast<unsigned>(SharedBytes(h, g4b::kBatched, h.blockSize));
     transport.kernelParams = transportArgs;
 
     if (h.graphExec == nullptr || h.graphPrecision != Precision(h)) {
@@ -655,7 +687,8 @@ void RunStaged(g4b_handle& h) {
             LaunchBatchedGraph(h, base, grid);
         } else {
             Check(g4b::LaunchZeroCounters(base.events, base.eventCount, base.run, h.stream), "zero counters");
-            Check(g4b::LaunchTransport(base, Precision(h), g4b::kBatched, grid, h.blockSize, SharedBytes(h), h.stream),
+            Check(g4b::LaunchTransport(base, Precision(h), g4b::kBatched, grid, h.blockSize,
+                                       SharedBytes(h, g4b::kBatched, h.blockSize), h.stream),
                   "transport launch");
         }
         h.launchCount += 2;
@@ -670,7 +703,8 @@ void RunStaged(g4b_handle& h) {
             p.photonEnd = event.photonEnd;
             const std::uint32_t photons{event.photonEnd - event.photonBegin};
             const unsigned grid{(photons + h.blockSize - 1U) / h.blockSize};
-            Check(g4b::LaunchTransport(p, Precision(h), g4b::kPlain, grid, h.blockSize, SharedBytes(h), h.stream),
+            Check(g4b::LaunchTransport(p, Precision(h), g4b::kPlain, grid, h.blockSize,
+                                       SharedBytes(h, g4b::kPlain, h.blockSize), h.stream),
                   "transport launch");
             ++h.launchCount;
         }
@@ -1094,7 +1128,7 @@ int g4b_create(const g4b_config* config, g4b_handle** outHandle) {
         Check(cudaEventCreateWithFlags(&handle->metadataReadyEvent, cudaEventDisableTiming), "cudaEventCreate");
         handle->blockSize = config->block_size != 0 ? config->block_size : 256;
         handle->blocksPerSM = config->blocks_per_sm;
-        handle->chunk = config->chunk_photons != 0 ? config->chunk_photons : 512;
+        handle->chunk = RoundChunk(config->chunk_photons != 0 ? config->chunk_photons : 512);
         *outHandle = handle.release();
     });
 }
@@ -1271,7 +1305,7 @@ int g4b_autotune(g4b_handle* h, const uint32_t* blockSizes, uint32_t nBlockSizes
         }
         Check(cudaSetDevice(h->device), "cudaSetDevice");
         const std::vector<std::uint32_t> defaultBlocks{128, 256};
-        const std::vector<std::uint32_t> defaultChunks{64, 128, 256, 512, 1024, 2048};
+        const std::vector<std::uint32_t> defaultChunks{128, 512, 2048};
         std::vector<std::uint32_t> blocks(blockSizes, blockSizes + (blockSizes != nullptr ? nBlockSizes : 0));
         std::vector<std::uint32_t> chunks(chunkSizes, chunkSizes + (chunkSizes != nullptr ? nChunkSizes : 0));
         if (blocks.empty()) blocks = defaultBlocks;
@@ -1286,18 +1320,20 @@ int g4b_autotune(g4b_handle* h, const uint32_t* blockSizes, uint32_t nBlockSizes
                 Throw(G4B_ERR_INVALID_ARGUMENT, "autotune block sizes must be multiples of 32 up to 256");
             }
             int maxBlocks{0};
-            Check(g4b::TransportOccupancy(Precision(*h), g4b::kBatched, static_cast<int>(block), SharedBytes(*h), &maxBlocks),
+            Check(g4b::TransportOccupancy(Precision(*h), g4b::kBatched, static_cast<int>(block),
+                                          SharedBytes(*h, g4b::kBatched, block), &maxBlocks),
                   "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
             maxBlocks = std::max(maxBlocks, 1);
             std::vector<std::uint32_t> perSM{static_cast<std::uint32_t>(maxBlocks)};
             if (maxBlocks > 1) {
-                perSM.push_back(static_cast<std::uint32_t>(maxBlocks / 2));
+                perSM.push_back(static_cast<std::uint32_t>(maxBlocks - 1));
             }
             for (const auto blocksPerSM : perSM) {
-                for (const auto chunk : chunks) {
-                    if (chunk == 0) {
+                for (const auto requested : chunks) {
+                    if (requested == 0) {
                         continue;
                     }
+                    const std::uint32_t chunk{RoundChunk(requested)};
                     h->blockSize = block;
                     h->blocksPerSM = blocksPerSM;
                     h->chunk = chunk;
@@ -1307,7 +1343,8 @@ int g4b_autotune(g4b_handle* h, const uint32_t* blockSizes, uint32_t nBlockSizes
                     for (std::uint32_t r{}; r < repeats + 1; ++r) {
                         Check(g4b::LaunchZeroCounters(p.events, p.eventCount, p.run, h->stream), "zero counters");
                         Check(cudaEventRecord(h->kernelTimer.start, h->stream), "cudaEventRecord");
-                        Check(g4b::LaunchTransport(p, Precision(*h), g4b::kBatched, grid, block, SharedBytes(*h), h->stream),
+                        Check(g4b::LaunchTransport(p, Precision(*h), g4b::kBatched, grid, block,
+                                                   SharedBytes(*h, g4b::kBatched, block), h->stream),
                               "transport launch");
                         Check(cudaEventRecord(h->kernelTimer.stop, h->stream), "cudaEventRecord");
                         Check(cudaEventSynchronize(h->kernelTimer.stop), "cudaEventSynchronize");

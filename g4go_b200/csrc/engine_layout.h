@@ -66,6 +66,12 @@ struct PackedVolume {
     std::uint8_t coincidentFaces; // bit f: face f = 2*axis + side touches another volume
     std::uint8_t mayCoincide;     // Volume::mayHaveCoincidentBoundary
     std::uint32_t sensorID;       // kInvalidID if not a sensor
+    // Boxes a ray starting inside this volume can cross first: itself and its
+    // daughters (bit b = volume b), in ascending order.
+    unsigned long long traceMask;
+    // Boxes whose faces can coincide with this volume's: itself and every
+    // volume it shares a coincident face with.
+    unsigned long long neighbourMask;
 };
 
 struct PackedScene {
@@ -85,6 +91,13 @@ struct PackedScene {
 };
 
 static_assert(sizeof(PackedScene) % 16 == 0, "scene blob must stay 16-byte aligned");
+
+// Per-warp photon queue in shared memory (batched form): 32 generated photons,
+// structure of arrays so that lanes reading different entries hit different
+// banks. Fields: position, direction, polarization (3 each), energy in the
+// transport type; time in double; eventID, photonID, volume, event index, slot.
+constexpr std::uint32_t kQueueBytesFP32 = 10U * 32U * 4U + 32U * 8U + 5U * 32U * 4U;  // 2176
+constexpr std::uint32_t kQueueBytesFP64 = 10U * 32U * 8U + 32U * 8U + 5U * 32U * 4U;  // 3456
 
 // Per-event counters (DeviceEventTransportStats, OptiXDeviceData.cuh:159-167),
 // padded to 64 bytes.
@@ -141,7 +154,7 @@ struct LaunchParams {
     std::uint32_t photonEnd;               // one past the last
     std::uint32_t emissionBegin;           // plain form: first emission of the event
     std::uint32_t emissionEnd;
-    std::uint32_t chunk;                   // batched form: photons per queue take
+    std::uint32_t chunk;                   // batched form: photons per queue take (multiple of 32)
     unsigned long long seed;
     std::uint32_t maxBounce;
     float epsilon;

@@ -2,9 +2,9 @@
 //
 // TransportBatched: one persistent launch per batch. Every warp pulls chunks
 // of flattened photon indices from a device work queue (one atomic ticket per
-// chunk) and refills each lane as soon as its photon ends, so warps stay full
-// while histories of a few to thousands of bounces finish at different
-// times. Gensteps are read as 8 x 16-byte loads; the scene lives in shared
+// chunk), generates them 32 at a time into a shared-memory photon queue, and
+// refills any idle lane from that queue in every iteration, so warps stay full
+// while histories of a few to thousands of bounces finish at different times. Gensteps are read as 8 x 16-byte loads; the scene lives in shared
 // memory; detections are compacted with one atomic per warp into a
 // structure-of-arrays hit buffer; event counters accumulate per lane and are
 // flushed once per event change.
@@ -173,6 +173,57 @@ __device__ __forceinline__ void RecordFate(const LaunchParams& p, std::uint32_t 
     }
 }
 
+// The shared-memory photon queue of one warp (layout sizes kQueueBytesFP32/64).
+template<class R>
+struct WarpQueue {
+    R positionX[32], positionY[32], positionZ[32];
+    R directionX[32], directionY[32], directionZ[32];
+    R polarizationX[32], polarizationY[32], polarizationZ[32];
+    R energy[32];
+    double time[32];
+    std::uint32_t eventID[32], photonID[32], volume[32], eventIndex[32], slot[32];
+
+    __device__ __forceinline__ void Put(unsigned k, const Photon<R>& photon) {
+        positionX[k] = photon.position.x;
+        positionY[k] = photon.position.y;
+        positionZ[k] = photon.position.z;
+        directionX[k] = photon.direction.x;
+        directionY[k] = photon.direction.y;
+        directionZ[k] = photon.direction.z;
+        polarizationX[k] = photon.polarization.x;
+        polarizationY[k] = photon.polarization.y;
+        polarizationZ[k] = photon.polarization.z;
+        energy[k] = photon.energy;
+        time[k] = photon.time;
+        eventID[k] = photon.eventID;
+        photonID[k] = photon.photonID;
+        volume[k] = photon.volume;
+        eventIndex[k] = photon.eventIndex;
+        slot[k] = photon.slot;
+    }
+    __device__ __forceinline__ void Take(unsigned k, Photon<R>& photon) const {
+        photon.position = {positionX[k], positionY[k], positionZ[k]};
+        photon.direction = {directionX[k], directionY[k], directionZ[k]};
+        photon.polarization = {polarizationX[k], polarizationY[k], polarizationZ[k]};
+        photon.energy = energy[k];
+        photon.time = time[k];
+        photon.eventID = eventID[k];
+        photon.photonID = photonID[k];
+        photon.volume = volume[k];
+        photon.eventIndex = eventIndex[k];
+        photon.slot = slot[k];
+        photon.bounce = 0U;
+    }
+};
+static_assert(sizeof(WarpQueue<float>) == kQueueBytesFP32, "queue layout");
+static_assert(sizeof(WarpQueue<double>) == kQueueBytesFP64, "queue layout");
+
+// Persistent transport. Each warp owns a 32-entry photon queue in shared
+// memory. When the queue is empty and a lane needs a photon, the whole warp
+// takes the next 32 flattened photon indices of its chunk (one atomic on the
+// device work queue per chunk) and generates them together, so generation
+// runs with every lane busy; idle lanes then refill from the queue in every
+// iteration at the cost of a few shared-memory loads.
 template<class R>
 __global__ void __launch_bounds__(256) TransportBatched(const LaunchParams p) {
     LoadScene(p);
@@ -182,11 +233,15 @@ __global__ void __launch_bounds__(256) TransportBatched(const LaunchParams p) {
     const unsigned lanesBelow{(1U << lane) - 1U};
     const R epsilon{R(p.epsilon)};
     const std::uint32_t totalPhotons{p.photonEnd - p.photonBegin};
+    WarpQueue<R>& queue{*reinterpret_cast<WarpQueue<R>*>(gShared + ((p.sceneBytes + 15U) & ~15U) +
+                                                         (threadIdx.x >> 5U) * sizeof(WarpQueue<R>))};
 
     std::uint32_t chunkNext{0U};
     std::uint32_t chunkEnd{0U};
     std::uint32_t cursor{0U};
-    bool queueDone{false};
+    std::uint32_t queueHead{0U};
+    std::uint32_t queueCount{0U};
+    bool workDone{false};
     bool alive{false};
     Photon<R> photon{};
     LaneCounters counters{};
@@ -197,51 +252,71 @@ __global__ void __launch_bounds__(256) TransportBatched(const LaunchParams p) {
     std::uint32_t coincidentHits{0U};
 
     for (;;) {
-        // Refill: lanes without a photon take the next indices of the warp's
-        // chunk; an exhausted chunk is replaced by one atomic on the ticket.
         unsigned need{__ballot_sync(kFullMask, !alive)};
-        while (need != 0U && !queueDone) {
-            if (chunkNext >= chunkEnd) {
-                std::uint32_t start{0U};
-                if (lane == 0U) {
-                    start = atomicAdd(&p.run->workTicket, p.chunk);
-                }
-                start = __shfl_sync(kFullMask, start, 0);
-                if (start >= totalPhotons) {
-                    queueDone = true;
+        while (need != 0U) {
+            if (queueHead == queueCount) {
+                if (workDone) {
                     break;
                 }
-                chunkNext = p.photonBegin + start;
-                chunkEnd = p.photonBegin + min(start + p.chunk, totalPhotons);
-                cursor = FindEmission(p.emissionOffsets, p.emissionBegin, p.emissionEnd, chunkNext);
+                // Refill the queue: the warp generates its next 32 photons.
+                if (chunkNext >= chunkEnd) {
+                    std::uint32_t start{0U};
+                    if (lane == 0U) {
+                        start = atomicAdd(&p.run->workTicket, p.chunk);
+                    }
+                    start = __shfl_sync(kFullMask, start, 0);
+                    if (start >= totalPhotons) {
+                        workDone = true;
+                        break;
+                    }
+                    chunkNext = p.photonBegin + start;
+                    chunkEnd = p.photonBegin + min(start + p.chunk, totalPhotons);
+                    cursor = FindEmission(p.emissionOffsets, p.emissionBegin, p.emissionEnd, chunkNext);
+                }
+                const std::uint32_t available{chunkEnd - chunkNext};
+                const bool has{lane < available};
+                std::uint32_t e{cursor};
+                bool valid{false};
+                Photon<R> fresh{};
+                if (has) {
+                    const std::uint32_t slot{chunkNext + lane};
+                    while (__ldg(p.emissionOffsets + e + 1U) <= slot) {
+                        ++e;
+                    }
+                    Emission emission;
+                    LoadEmission(p.emissions, e, emission);
+                    const std::uint32_t local{slot - __ldg(p.emissionOffsets + e)};
+                    const std::uint32_t eventIndex{__ldg(p.emissionEventIndices + e)};
+                    GeneratePhoton<R>(scene, pool, emission, emission.FirstPhotonID() + local, p.seed, fresh);
+                    fresh.eventIndex = eventIndex;
+                    fresh.slot = (p.slotBase != nullptr) ? __ldg(p.slotBase + e) + local : slot;
+                    valid = StartPhoton(fresh);
+                    if (!valid) {
+                        atomicAdd(&p.events[eventIndex].invalid, 1ULL);
+                        RecordFate(p, fresh.slot, kInvalid, 0U, fresh.time);
+                    }
+                }
+                const unsigned hasMask{__ballot_sync(kFullMask, has)};
+                cursor = __shfl_sync(kFullMask, e, 31 - __clz(static_cast<int>(hasMask)));
+                chunkNext += min(available, 32U);
+                const unsigned validMask{__ballot_sync(kFullMask, valid)};
+                if (valid) {
+                    queue.Put(static_cast<unsigned>(__popc(validMask & lanesBelow)), fresh);
+                }
+                __syncwarp();
+                queueHead = 0U;
+                queueCount = static_cast<std::uint32_t>(__popc(validMask));
+                continue;
             }
-            const std::uint32_t available{chunkEnd - chunkNext};
+            const std::uint32_t available{queueCount - queueHead};
             const std::uint32_t rank{static_cast<std::uint32_t>(__popc(need & lanesBelow))};
             const bool take{((need >> lane) & 1U) != 0U && rank < available};
-            const std::uint32_t taken{min(static_cast<std::uint32_t>(__popc(need)), available)};
-            std::uint32_t e{cursor};
             if (take) {
-                const std::uint32_t slot{chunkNext + rank};
-                while (__ldg(p.emissionOffsets + e + 1U) <= slot) {
-                    ++e;
-                }
-                Emission emission;
-                LoadEmission(p.emissions, e, emission);
-                const std::uint32_t local{slot - __ldg(p.emissionOffsets + e)};
-                const std::uint32_t eventIndex{__ldg(p.emissionEventIndices + e)};
-                counters.Switch(eventIndex, p.events);
-                GeneratePhoton<R>(scene, pool, emission, emission.FirstPhotonID() + local, p.seed, photon);
-                photon.eventIndex = eventIndex;
-                photon.slot = (p.slotBase != nullptr) ? __ldg(p.slotBase + e) + local : slot;
-                alive = StartPhoton(photon);
-                if (!alive) {
-                    ++counters.invalid;
-                    RecordFate(p, photon.slot, kInvalid, 0U, photon.time);
-                }
+                queue.Take(queueHead + rank, photon);
+                counters.Switch(photon.eventIndex, p.events);
+                alive = true;
             }
-            const unsigned takeMask{__ballot_sync(kFullMask, take)};
-            cursor = __shfl_sync(kFullMask, e, 31 - __clz(static_cast<int>(takeMask)));
-            chunkNext += taken;
+            queueHead += min(static_cast<std::uint32_t>(__popc(need)), available);
             need = __ballot_sync(kFullMask, !alive);
         }
         if (__ballot_sync(kFullMask, alive) == 0U) {
@@ -266,6 +341,7 @@ __global__ void __launch_bounds__(256) TransportBatched(const LaunchParams p) {
                 alive = false;
             }
         }
+        __syncwarp();
     }
     counters.Flush(p.events);
     FlushRunCounters(p, laneBounces, coincidentTraces, coincidentHits, lane);

@@ -203,7 +203,8 @@ typedef struct g4b_config {
     uint64_t hit_capacity;           /* device hit-buffer rows; 0 -> photons of the batch */
     uint32_t block_size;             /* 0 -> autotuned/default (256) */
     uint32_t blocks_per_sm;          /* 0 -> from occupancy */
-    uint32_t chunk_photons;          /* photons a warp takes from the work queue at a time; 0 -> 512 */
+    uint32_t chunk_photons;          /* photons a warp takes from the work queue at a time (rounded up to
+                                        a multiple of 32); 0 -> 512 */
     uint32_t use_cuda_graph;         /* 1 -> batched launches replay a captured graph */
     uint32_t record_photon_fates;    /* 1 -> keep a per-photon fate/bounce/time record (diagnostics) */
     uint32_t reserved[7];
@@ -357,8 +358,8 @@ int g4b_photon_fates(g4b_handle* handle, uint32_t* fate, double* time_ns, uint64
 
 /* Launch-shape autotuner: times the staged batch (the last one passed to
  * g4b_enqueue, which must have completed) under every candidate
- * block size x blocks per SM x chunk size, keeps the fastest in the handle
- * and reports it. Candidate lists may be NULL for the built-in sweep. */
+ * block size x blocks per SM x queue chunk size, keeps the fastest in the
+ * handle and reports it. Candidate lists may be NULL for the built-in sweep. */
 typedef struct g4b_tune_result {
     uint32_t block_size;
     uint32_t blocks_per_sm;
