@@ -198,6 +198,7 @@ def bench_ours(args, world, rank, local):
 
     from g4go_b200 import DETECTION_DTYPE, PhotonTransportConfig, TransportHost, scenes
     from g4go_b200 import _abi
+    from g4go_b200.multigpu import max_over_ranks
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -263,9 +264,7 @@ def bench_ours(args, world, rank, local):
     sampler.stop()
     elapsed_ms = start.elapsed_time(stop)
     if world > 1:
-        t = torch.tensor([elapsed_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+        elapsed_ms = max_over_ranks(elapsed_ms)
     ms_per_step = elapsed_ms / args.steps
     value = photons * world / (ms_per_step / 1000.0)
 
@@ -299,9 +298,7 @@ def bench_ours(args, world, rank, local):
         torch.cuda.synchronize()
         e2e_ms = e2e_start.elapsed_time(e2e_stop) / e2e_steps
         if world > 1:
-            t = torch.tensor([e2e_ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+            e2e_ms = max_over_ranks(e2e_ms)
         e2e = {"value": photons * world / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms}
         del detections, staged, pinned_batch

@@ -265,6 +265,26 @@ class TuneResult(C.Structure):
     ]
 
 
+class GradientRequest(C.Structure):
+    _fields_ = [
+        ("rindex_material_id", C.c_uint32),
+        ("abs_length_material_id", C.c_uint32),
+        ("reflectivity_surface_id", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
+class Gradients(C.Structure):
+    _fields_ = [
+        ("detected", C.c_uint64),
+        ("replay_mismatches", C.c_uint64),
+        ("mean_time_ns", C.c_double),
+        ("d_detected", C.c_double * 4),
+        ("d_mean_time_ns", C.c_double * 4),
+        ("kernel_ms", C.c_double),
+    ]
+
+
 class SynthParams(C.Structure):
     _fields_ = [
         ("event_count", C.c_uint32),
@@ -316,6 +336,7 @@ SIGNATURES = {
     "g4b_get_stream": (_I32, [_VP, C.POINTER(_VP)]),
     "g4b_photon_fates": (_I32, [_VP, _PU32, _PD, _U64, _PU64]),
     "g4b_autotune": (_I32, [_VP, _PU32, _U32, _PU32, _U32, _U32, C.POINTER(TuneResult)]),
+    "g4b_gradients": (_I32, [_VP, C.POINTER(GradientRequest), C.POINTER(Gradients)]),
     "g4b_eval_fresnel": (_I32, [_I32, _U32, _U32, _PD, _PD, _PD, _PD, _PD, _PD]),
     "g4b_eval_lambertian": (_I32, [_I32, _U32, _U32, _PD, _PD, _PD, _PD]),
     "g4b_eval_math": (_I32, [_I32, _U32, _U32, _PF, _PF]),

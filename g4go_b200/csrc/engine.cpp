@@ -168,7 +168,7 @@ struct g4b_handle {
     DeviceBuffer dEmissions, dOffsets, dEventIndices, dSlotBase, dEvents, dRun;
     DeviceBuffer dHits[kHitColumns];
     std::uint64_t hitCapacity{0};
-    DeviceBuffer dBitmap, dPrefix, dBlockSums, dDetections, dFate, dFateTime;
+    DeviceBuffer dBitmap, dPrefix, dBlockSums, dDetections, dFate, dFateTime, dGradient;
 
     // The staged batch (kept for g4b_relaunch) and the pending one.
     bool hasStaged{false};
@@ -1371,6 +1371,61 @@ int g4b_autotune(g4b_handle* h, const uint32_t* blockSizes, uint32_t nBlockSizes
         if (result != nullptr) {
             *result = best;
         }
+    });
+}
+
+int g4b_gradients(g4b_handle* h, const g4b_gradient_request* request, g4b_gradient_result* result) {
+    if (h == nullptr) {
+        gHandlelessError = "null handle";
+        return G4B_ERR_INVALID_ARGUMENT;
+    }
+    return Guard(h, [&]() {
+        if (request == nullptr || result == nullptr) {
+            Throw(G4B_ERR_INVALID_ARGUMENT, "null argument");
+        }
+        if (h->busy) {
+            Throw(G4B_ERR_LOGIC, "gradients need the pending batch completed first");
+        }
+        if (!h->hasStaged || h->photonCount == 0) {
+            Throw(G4B_ERR_LOGIC, "gradients need a completed batch with photons");
+        }
+        if (h->usesSlotBase) {
+            Throw(G4B_ERR_UNSUPPORTED, "gradients of a batch the plain form regrouped by event are not supported");
+        }
+        if (request->rindex_material_id != kInvalidID && request->rindex_material_id >= h->materialCount) {
+            Throw(G4B_ERR_INVALID_ARGUMENT, "gradient request names an unknown material");
+        }
+        if (request->abs_length_material_id != kInvalidID && request->abs_length_material_id >= h->materialCount) {
+            Throw(G4B_ERR_INVALID_ARGUMENT, "gradient request names an unknown material");
+        }
+        Check(cudaSetDevice(h->device), "cudaSetDevice");
+        const std::uint64_t hits{std::min<std::uint64_t>(h->hRun.As<RunCounters>()->hitCount, h->hitCapacity)};
+        h->dGradient.Ensure(sizeof(g4b::GradientSums), "cudaMalloc gradient sums");
+        Check(cudaMemsetAsync(h->dGradient.pointer, 0, sizeof(g4b::GradientSums), h->stream), "cudaMemsetAsync");
+        const LaunchParams p{BaseParams(*h)};
+        Check(cudaEventRecord(h->kernelTimer.start, h->stream), "cudaEventRecord");
+        Check(g4b::LaunchGradientReplay(p, Precision(*h), request->rindex_material_id, request->abs_length_material_id,
+                                        request->reflectivity_surface_id, hits, SceneSharedBytes(*h),
+                                        h->dGradient.As<g4b::GradientSums>(), h->stream),
+              "gradient replay");
+        Check(cudaEventRecord(h->kernelTimer.stop, h->stream), "cudaEventRecord");
+        ++h->launchCount;
+        g4b::GradientSums sums{};
+        Check(cudaMemcpyAsync(&sums, h->dGradient.pointer, sizeof(sums), cudaMemcpyDeviceToHost, h->stream),
+              "cudaMemcpyAsync gradient sums");
+        Check(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+        // N = sum 1; mean t = sum t / N; dN = sum S; d(mean t) = (sum (t S + dt) - mean t * sum S) / N.
+        g4b_gradient_result out{};
+        out.detected = static_cast<std::uint64_t>(sums.detected);
+        out.replay_mismatches = sums.mismatches;
+        const double n{sums.detected};
+        out.mean_time_ns = n > 0.0 ? sums.time / n : 0.0;
+        for (int j{}; j < 4; ++j) {
+            out.d_detected[j] = sums.score[j];
+            out.d_mean_time_ns[j] = n > 0.0 ? (sums.timeScore[j] - out.mean_time_ns * sums.score[j]) / n : 0.0;
+        }
+        out.kernel_ms = h->kernelTimer.Milliseconds();
+        *result = out;
     });
 }
 

@@ -123,6 +123,17 @@ struct RunCounters {
     unsigned long long reserved[3];
 };
 
+// Sums of the gradient replay over the detected photons, FP64. Parameter j:
+// 0 refractive index, 1 absorption length, 2 reflectivity, 3 decay time.
+struct GradientSums {
+    double detected;       // N
+    double time;           // sum of arrival times
+    double score[4];       // sum of S_j (score + pathwise log-probability terms)
+    double timeScore[4];   // sum of t S_j + dt/dtheta_j
+    unsigned long long mismatches;  // detected photons the replay did not reproduce
+    unsigned long long reserved;
+};
+
 // Compacted hits, structure of arrays, `capacity` rows each.
 struct HitColumns {
     float* positionX;

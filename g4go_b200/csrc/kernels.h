@@ -37,6 +37,14 @@ cudaError_t LaunchOrderHits(const HitColumns& hits, unsigned long long count, st
                             std::uint32_t* bitmap, std::uint32_t* prefix, std::uint32_t* blockSums,
                             void* detectionsOut, bool ordered, cudaStream_t stream);
 
+// Gradient replay over the `count` detected photons of the last transport:
+// each one is regenerated and re-transported from its RNG counters with dual
+// numbers, and its score and pathwise terms are summed into `sums`.
+cudaError_t LaunchGradientReplay(const LaunchParams& params, int precision, std::uint32_t indexMaterial,
+                                 std::uint32_t absMaterial, std::uint32_t reflectivitySurface,
+                                 unsigned long long count, std::size_t sharedBytes, GradientSums* sums,
+                                 cudaStream_t stream);
+
 cudaError_t LaunchEvalFresnel(int precision, std::uint32_t n, const double* in, double* out, cudaStream_t stream);
 cudaError_t LaunchEvalLambertian(int precision, std::uint32_t n, const double* in, double* out, cudaStream_t stream);
 cudaError_t LaunchEvalMath(std::uint32_t kind, std::uint32_t n, const float* in, float* out, cudaStream_t stream);

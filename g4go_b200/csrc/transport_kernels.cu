@@ -155,7 +155,7 @@ __device__ __forceinline__ void FlushRunCounters(const LaunchParams& p, unsigned
 template<class R>
 __device__ __forceinline__ bool StartPhoton(Photon<R>& photon) {
     const R lengthSquared{Dot(photon.direction, photon.direction)};
-    if (!(photon.energy > R(0)) || !isfinite(photon.energy) || !(lengthSquared > R(0)) || !isfinite(lengthSquared)) {
+    if (!(photon.energy > R(0)) || !IsFinite(photon.energy) || !(lengthSquared > R(0)) || !IsFinite(lengthSquared)) {
         return false;
     }
     photon.direction = NormalizeChecked(photon.direction);
@@ -224,8 +224,20 @@ static_assert(sizeof(WarpQueue<double>) == kQueueBytesFP64, "queue layout");
 // device work queue per chunk) and generates them together, so generation
 // runs with every lane busy; idle lanes then refill from the queue in every
 // iteration at the cost of a few shared-memory loads.
+// Resident 256-thread blocks per SM the compiler must allow: for FP32 three
+// (at most 85 registers), which measured faster than the unconstrained
+// allocation despite a few spills; FP64 keeps the compiler's choice.
 template<class R>
-__global__ void __launch_bounds__(256) TransportBatched(const LaunchParams p) {
+struct BatchedMinBlocks {
+    static constexpr int value = 3;
+};
+template<>
+struct BatchedMinBlocks<double> {
+    static constexpr int value = 1;
+};
+
+template<class R>
+__global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatched(const LaunchParams p) {
     LoadScene(p);
     const PackedScene& scene{*reinterpret_cast<const PackedScene*>(gShared)};
     const float* pool{PoolOf(scene)};
@@ -287,7 +299,7 @@ __global__ void __launch_bounds__(256) TransportBatched(const LaunchParams p) {
                     LoadEmission(p.emissions, e, emission);
                     const std::uint32_t local{slot - __ldg(p.emissionOffsets + e)};
                     const std::uint32_t eventIndex{__ldg(p.emissionEventIndices + e)};
-                    GeneratePhoton<R>(scene, pool, emission, emission.FirstPhotonID() + local, p.seed, fresh);
+                    GeneratePhoton<R>(scene, pool, emission, emission.FirstPhotonID() + local, p.seed, NoGradient(), fresh);
                     fresh.eventIndex = eventIndex;
                     fresh.slot = (p.slotBase != nullptr) ? __ldg(p.slotBase + e) + local : slot;
                     valid = StartPhoton(fresh);
@@ -326,7 +338,7 @@ __global__ void __launch_bounds__(256) TransportBatched(const LaunchParams p) {
         std::uint32_t result{kContinue};
         StepExtras extras{0U, 0U, 0U, 0U};
         if (alive) {
-            result = StepPhoton<R>(scene, pool, photon, p.seed, p.maxBounce, epsilon, extras);
+            result = StepPhoton<R>(scene, pool, photon, p.seed, p.maxBounce, epsilon, extras, NoGradient());
         }
         WriteHits(alive && result == kDetected, photon, extras.sensorID, p, lane);
         if (alive) {
@@ -371,7 +383,7 @@ __global__ void __launch_bounds__(256) TransportPlain(const LaunchParams p) {
         const std::uint32_t local{slot - __ldg(p.emissionOffsets + e)};
         const std::uint32_t eventIndex{__ldg(p.emissionEventIndices + e)};
         counters.eventIndex = eventIndex;
-        GeneratePhoton<R>(scene, pool, emission, emission.FirstPhotonID() + local, p.seed, photon);
+        GeneratePhoton<R>(scene, pool, emission, emission.FirstPhotonID() + local, p.seed, NoGradient(), photon);
         photon.eventIndex = eventIndex;
         photon.slot = (p.slotBase != nullptr) ? __ldg(p.slotBase + e) + local : slot;
         alive = StartPhoton(photon);
@@ -384,7 +396,7 @@ __global__ void __launch_bounds__(256) TransportPlain(const LaunchParams p) {
         std::uint32_t result{kContinue};
         StepExtras extras{0U, 0U, 0U, 0U};
         if (alive) {
-            result = StepPhoton<R>(scene, pool, photon, p.seed, p.maxBounce, epsilon, extras);
+            result = StepPhoton<R>(scene, pool, photon, p.seed, p.maxBounce, epsilon, extras, NoGradient());
         }
         WriteHits(alive && result == kDetected, photon, extras.sensorID, p, lane);
         if (alive) {
@@ -402,6 +414,76 @@ __global__ void __launch_bounds__(256) TransportPlain(const LaunchParams p) {
     }
     counters.Flush(p.events);
     FlushRunCounters(p, laneBounces, coincidentTraces, coincidentHits, lane);
+}
+
+// Gradient replay: one thread per detected photon. The photon is regenerated
+// from its genstep and RNG counters and transported again with Dual<R>, which
+// repeats the forward history exactly (same values, same choices) while
+// carrying d/dn; the score terms of every discrete choice accumulate along the
+// way. Per-photon results are reduced per warp in FP64 and added to `sums`.
+template<class R>
+__global__ void __launch_bounds__(128) GradientReplay(const LaunchParams p, GradientTargets targets,
+                                                      unsigned long long count, GradientSums* sums) {
+    using D = Dual<R>;
+    LoadScene(p);
+    const PackedScene& scene{*reinterpret_cast<const PackedScene*>(gShared)};
+    const float* pool{PoolOf(scene)};
+    const unsigned long long i{blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x};
+    double values[11]{};
+    if (i < count) {
+        const std::uint32_t slot{p.hits.slot[i]};
+        const std::uint32_t e{FindEmission(p.emissionOffsets, 0U, p.emissionCount, slot)};
+        Emission emission;
+        LoadEmission(p.emissions, e, emission);
+        const std::uint32_t local{slot - __ldg(p.emissionOffsets + e)};
+        Photon<D> photon{};
+        GeneratePhoton<D>(scene, pool, emission, emission.FirstPhotonID() + local, p.seed, targets, photon);
+        photon.slot = slot;
+        std::uint32_t result{kInvalid};
+        StepExtras extras{0U, 0U, 0U, 0U};
+        if (StartPhoton(photon)) {
+            const D epsilon{p.epsilon};
+            do {
+                result = StepPhoton<D>(scene, pool, photon, p.seed, p.maxBounce, epsilon, extras, targets);
+            } while (result == kContinue);
+        }
+        const bool reproduced{result == kDetected && extras.sensorID == p.hits.sensorID[i] &&
+                              static_cast<float>(photon.time) == p.hits.time[i]};
+        if (reproduced) {
+            const double t{photon.time};
+            const double score[4]{photon.tangents.scoreIndex, photon.tangents.scoreAbsLength,
+                                  photon.tangents.scoreReflectivity, 0.0};
+            const double dt[4]{photon.tangents.dTimeDIndex, 0.0, 0.0, photon.tangents.dTimeDDecay};
+            values[0] = 1.0;
+            values[1] = t;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                values[2 + j] = score[j];
+                values[6 + j] = t * score[j] + dt[j];
+            }
+        } else {
+            values[10] = 1.0;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 11; ++k) {
+#pragma unroll
+        for (int offset = 16; offset > 0; offset >>= 1) {
+            values[k] += __shfl_down_sync(kFullMask, values[k], offset);
+        }
+    }
+    if ((threadIdx.x & 31U) == 0U) {
+        atomicAdd(&sums->detected, values[0]);
+        atomicAdd(&sums->time, values[1]);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            atomicAdd(&sums->score[j], values[2 + j]);
+            atomicAdd(&sums->timeScore[j], values[6 + j]);
+        }
+        if (values[10] != 0.0) {
+            atomicAdd(&sums->mismatches, static_cast<unsigned long long>(values[10]));
+        }
+    }
 }
 
 __global__ void ZeroCounters(EventCounters* events, std::uint32_t eventCount, RunCounters* run) {
@@ -704,6 +786,30 @@ cudaError_t LaunchOrderHits(const HitColumns& hits, unsigned long long count, st
     }
     ScatterDetections<<<BlocksFor(count, 256U), 256, 0, stream>>>(hits, count, bitmap, prefix, ordered,
                                                                   static_cast<float4*>(detectionsOut));
+    return cudaGetLastError();
+}
+
+cudaError_t LaunchGradientReplay(const LaunchParams& params, int precision, std::uint32_t indexMaterial,
+                                 std::uint32_t absMaterial, std::uint32_t reflectivitySurface,
+                                 unsigned long long count, std::size_t sharedBytes, GradientSums* sums,
+                                 cudaStream_t stream) {
+    const GradientTargets targets{indexMaterial, absMaterial, reflectivitySurface};
+    const void* kernel{precision == kFP64 ? reinterpret_cast<const void*>(&GradientReplay<double>)
+                                          : reinterpret_cast<const void*>(&GradientReplay<float>)};
+    cudaError_t error{cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(sharedBytes))};
+    if (error != cudaSuccess) {
+        return error;
+    }
+    if (count == 0ULL) {
+        return cudaSuccess;
+    }
+    const unsigned blocks{static_cast<unsigned>((count + 127ULL) / 128ULL)};
+    if (precision == kFP64) {
+        GradientReplay<double><<<blocks, 128, sharedBytes, stream>>>(params, targets, count, sums);
+    } else {
+        GradientReplay<float><<<blocks, 128, sharedBytes, stream>>>(params, targets, count, sums);
+    }
     return cudaGetLastError();
 }
 

@@ -66,13 +66,15 @@ class DetectorParameters:
     wrapper_reflectivity: float = 0.95
     sipm_efficiency: float = 0.3
     world_half_mm: float = 50.0
+    coupling_half_xy_mm: float | None = None  # grease and SiPM half width; None -> the crystal's
     emission_mean_nm: float = 420.0
     emission_sigma_nm: float = 20.0
 
 
-# Volume IDs and material IDs of the detector scene.
+# Volume, material and surface IDs of the detector scene.
 WORLD, CRYSTAL, GREASE, SIPM = 0, 1, 2, 3
 MAT_AIR, MAT_CRYSTAL, MAT_GREASE, MAT_SILICON = 0, 1, 2, 3
+SURF_WRAPPER, SURF_COATING, SURF_CATHODE = 0, 1, 2
 
 
 def crystal_sipm_scene(params: DetectorParameters | None = None) -> Scene:
@@ -115,12 +117,14 @@ def crystal_sipm_scene(params: DetectorParameters | None = None) -> Scene:
     scene.add_volume(Volume("world", WORLD, MAT_AIR, INVALID_ID, INVALID_ID, INVALID_ID, (0.0, 0.0, 0.0), (w, w, w)))
     scene.add_volume(Volume("crystal", CRYSTAL, MAT_CRYSTAL, WORLD, INVALID_ID, INVALID_ID, (0.0, 0.0, 0.0), (hx, hy, hz)))
     g = p.grease_thickness_mm
+    cx = hx if p.coupling_half_xy_mm is None else p.coupling_half_xy_mm
+    cy = hy if p.coupling_half_xy_mm is None else p.coupling_half_xy_mm
     scene.add_volume(
-        Volume("grease", GREASE, MAT_GREASE, WORLD, INVALID_ID, INVALID_ID, (0.0, 0.0, hz + g / 2), (hx, hy, g / 2))
+        Volume("grease", GREASE, MAT_GREASE, WORLD, INVALID_ID, INVALID_ID, (0.0, 0.0, hz + g / 2), (cx, cy, g / 2))
     )
     s = p.sipm_thickness_mm
     scene.add_volume(
-        Volume("sipm", SIPM, MAT_SILICON, WORLD, cathode, 0, (0.0, 0.0, hz + g + s / 2), (hx, hy, s / 2))
+        Volume("sipm", SIPM, MAT_SILICON, WORLD, cathode, 0, (0.0, 0.0, hz + g + s / 2), (cx, cy, s / 2))
     )
     scene.add_surface_binding(SurfaceBinding(CRYSTAL, WORLD, wrapper))
     scene.add_surface_binding(SurfaceBinding(WORLD, CRYSTAL, coating))

@@ -453,6 +453,23 @@ class TransportHost:
         )
         return fate, time
 
+    PARAMETERS = ("rindex", "abs_length_mm", "reflectivity", "decay_time_ns")
+
+    def gradients(self, rindex_material: int = INVALID_ID, abs_length_material: int = INVALID_ID,
+                  reflectivity_surface: int = INVALID_ID) -> dict:
+        """d(detected)/d theta and d(mean arrival time)/d theta for the last completed batch."""
+        request = _abi.GradientRequest(rindex_material, abs_length_material, reflectivity_surface, 0)
+        result = _abi.Gradients()
+        self._check(self._lib.g4b_gradients(self._handle, C.byref(request), C.byref(result)))
+        return {
+            "detected": int(result.detected),
+            "mean_time_ns": float(result.mean_time_ns),
+            "d_detected": dict(zip(self.PARAMETERS, list(result.d_detected))),
+            "d_mean_time_ns": dict(zip(self.PARAMETERS, list(result.d_mean_time_ns))),
+            "replay_mismatches": int(result.replay_mismatches),
+            "kernel_ms": float(result.kernel_ms),
+        }
+
     def autotune(self, block_sizes: Sequence[int] = (), chunk_sizes: Sequence[int] = (), repeats: int = 2) -> dict:
         blocks = np.ascontiguousarray(block_sizes, dtype=np.uint32)
         chunks = np.ascontiguousarray(chunk_sizes, dtype=np.uint32)

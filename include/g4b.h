@@ -372,6 +372,41 @@ int g4b_autotune(g4b_handle* handle, const uint32_t* block_sizes, uint32_t n_blo
                  const uint32_t* chunk_sizes, uint32_t n_chunk_sizes, uint32_t repeats,
                  g4b_tune_result* result);
 
+/* --- Gradients (no counterpart in the reference) ---------------------------
+ * Derivatives of the detected count N and of the mean arrival time of the
+ * detected photons with respect to four parameters, for the batch last
+ * completed on this handle (same gensteps, same seed): a refractive index
+ * (of one material, constant RINDEX table), an absorption length (one
+ * material), a reflectivity (one surface) and the scintillation decay time
+ * (all scintillation gensteps). Each detected photon is regenerated and
+ * re-transported from its RNG counters with forward-mode dual numbers
+ * (pathwise derivatives through the step loop) while the score terms
+ * d log p / d theta of its discrete choices (Fresnel reflect/transmit,
+ * surface classification, survival of bulk absorption) accumulate; nothing
+ * of the forward trajectories is stored. FP32 replay for an FP32 handle with
+ * FP64 accumulation. Geometric discontinuities (a changed parameter moving a
+ * photon to another face) are not included. Batches the plain form regrouped
+ * by event are not supported. */
+typedef struct g4b_gradient_request {
+    uint32_t rindex_material_id;      /* G4B_INVALID_ID: no index derivative */
+    uint32_t abs_length_material_id;  /* G4B_INVALID_ID: none */
+    uint32_t reflectivity_surface_id; /* G4B_INVALID_ID: none */
+    uint32_t reserved;
+} g4b_gradient_request;
+
+/* Parameter order in the arrays: 0 refractive index, 1 absorption length
+ * (per mm), 2 reflectivity, 3 scintillation decay time (per ns). */
+typedef struct g4b_gradient_result {
+    uint64_t detected;
+    uint64_t replay_mismatches; /* detected photons the replay did not reproduce; 0 expected */
+    double mean_time_ns;
+    double d_detected[4];
+    double d_mean_time_ns[4];
+    double kernel_ms;
+} g4b_gradient_result;
+
+int g4b_gradients(g4b_handle* handle, const g4b_gradient_request* request, g4b_gradient_result* result);
+
 /* --- Device-evaluated boundary and math kernels ---------------------------
  * Run the transport's own device functions on caller inputs, so the boundary
  * unit cases of test/TestOpticalBoundaryPhysics.cxx:37-101 can be checked on
