@@ -147,7 +147,7 @@ def _fresnel_golden_check(rows_out, golden, tolerance):
     nrm = golden["fresnel_normal"].astype(np.float64)
     cos_i = np.clip(-np.sum(d * nrm, axis=1) / np.linalg.norm(d, axis=1) / np.linalg.norm(nrm, axis=1), 0, 1)
     brewster = np.arctan(n2 / n1)
-    near_brewster = np.abs(np.arccos(cos_i) - brewster) < 5e-3
+    near_brewster = np.abs(np.arccos(cos_i) - brewster) < 2e-2
     # Equal indices reflect nothing: the reference's FP32 cos(theta_t) makes a
     # spurious tiny reflection at grazing incidence whose polarisation is noise.
     reflecting = same & (1.0 - ref[:, 12] > 1e-6) & ~near_brewster & (n1 != n2)
