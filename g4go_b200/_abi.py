@@ -343,6 +343,7 @@ SIGNATURES = {
     "g4b_eval_uniform": (_I32, [_I32, _U32, _U64, _PU64, _PU32, _PU32, _PU32, _PF]),
     "g4b_host_alloc": (_I32, [C.c_size_t, C.POINTER(_VP)]),
     "g4b_host_free": (_I32, [_VP]),
+    "g4b_order_detections_static": (_I32, [_VP, _VP, _U64, _U32, _VP, _VP]),
     "g4b_abi_version": (_U32, []),
     "g4b_synth_electrons": (_I32, [C.POINTER(SynthParams), C.POINTER(_VP)]),
     "g4b_synth_isotropic_photons": (

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
@@ -1082,6 +1083,29 @@ void DeviceEval(int device, std::size_t inCount, const In* input, std::size_t ou
     cleanup();
 }
 
+// --- ordering without allocation ------------------------------------------
+//
+// g4b_order_detections_static must not allocate, so it reports failures by
+// status code with a message written into a buffer reserved on the thread's
+// first call, and keeps the scratch address of each device in a fixed table.
+
+static_assert(G4B_ORDER_STATIC_MAX_SLOTS == g4b::kStaticOrderMaxSlots,
+              "the header's slot limit must match the kernels' scratch size");
+constexpr std::size_t kStaticOrderMessageBytes{256};
+constexpr int kStaticOrderDevices{64};
+std::mutex gStaticOrderLock;
+std::uint32_t* gStaticOrderScratch[kStaticOrderDevices]{};
+
+int StaticOrderFailure(int code, const char* what, cudaError_t error = cudaSuccess) {
+    // the message stays below the reserved capacity, so no allocation
+    gHandlelessError.assign(what);
+    if (error != cudaSuccess) {
+        gHandlelessError.append(": ");
+        gHandlelessError.append(cudaGetErrorName(error));
+    }
+    return code;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1444,6 +1468,75 @@ int g4b_host_free(void* pointer) {
             Check(cudaFreeHost(pointer), "cudaFreeHost");
         }
     });
+}
+
+int g4b_order_detections_static(const g4b_photon_detection* unordered, const uint32_t* slots, uint64_t count,
+                                uint32_t slot_limit, g4b_photon_detection* ordered, void* stream) {
+    if (gHandlelessError.capacity() < kStaticOrderMessageBytes) {
+        try {
+            gHandlelessError.reserve(kStaticOrderMessageBytes);
+        } catch (const std::bad_alloc&) {
+            return G4B_ERR_CUDA;
+        }
+    }
+    if (slot_limit > G4B_ORDER_STATIC_MAX_SLOTS) {
+        return StaticOrderFailure(G4B_ERR_OVERFLOW,
+                                  "slot_limit exceeds G4B_ORDER_STATIC_MAX_SLOTS (16777216), the static scratch size");
+    }
+    if (count == 0) {
+        return G4B_OK;
+    }
+    if (count > slot_limit) {
+        return StaticOrderFailure(G4B_ERR_INVALID_ARGUMENT, "count exceeds slot_limit: keys must be unique and below it");
+    }
+    if (unordered == nullptr || slots == nullptr || ordered == nullptr) {
+        return StaticOrderFailure(G4B_ERR_INVALID_ARGUMENT, "null argument");
+    }
+    const auto in{reinterpret_cast<std::uintptr_t>(unordered)};
+    const auto out{reinterpret_cast<std::uintptr_t>(ordered)};
+    if (in % 16U != 0U || out % 16U != 0U || reinterpret_cast<std::uintptr_t>(slots) % 4U != 0U) {
+        return StaticOrderFailure(G4B_ERR_INVALID_ARGUMENT,
+                                  "records must be 16-byte aligned and slot keys 4-byte aligned");
+    }
+    const std::uintptr_t bytes{static_cast<std::uintptr_t>(count) * sizeof(g4b_photon_detection)};
+    if (in < out + bytes && out < in + bytes) {
+        return StaticOrderFailure(G4B_ERR_INVALID_ARGUMENT, "unordered and ordered records overlap");
+    }
+    int device{0};
+    cudaError_t error{cudaGetDevice(&device)};
+    if (error != cudaSuccess) {
+        cudaGetLastError();
+        return StaticOrderFailure(G4B_ERR_NO_DEVICE, "no current CUDA device", error);
+    }
+    if (device < 0 || device >= kStaticOrderDevices) {
+        return StaticOrderFailure(G4B_ERR_NO_DEVICE, "device ordinal beyond the scratch address table (64 devices)");
+    }
+    std::uint32_t* scratch{nullptr};
+    {
+        const std::lock_guard<std::mutex> lock{gStaticOrderLock};
+        if (gStaticOrderScratch[device] == nullptr) {
+            error = g4b::StaticOrderScratch(&gStaticOrderScratch[device]);
+            if (error != cudaSuccess) {
+                gStaticOrderScratch[device] = nullptr;
+                cudaGetLastError();
+                const bool noImage{error == cudaErrorNoKernelImageForDevice || error == cudaErrorInvalidDeviceFunction};
+                return StaticOrderFailure(noImage ? G4B_ERR_NO_DEVICE : G4B_ERR_CUDA,
+                                          "cudaGetSymbolAddress of the static scratch", error);
+            }
+        }
+        scratch = gStaticOrderScratch[device];
+    }
+    std::uint32_t rejected{0};
+    error = g4b::LaunchOrderRecordsStatic(unordered, slots, count, slot_limit, scratch, ordered, &rejected,
+                                          static_cast<cudaStream_t>(stream));
+    if (error != cudaSuccess) {
+        cudaGetLastError();
+        return StaticOrderFailure(G4B_ERR_CUDA, "static ordering", error);
+    }
+    if (rejected != 0U) {
+        return StaticOrderFailure(G4B_ERR_INVALID_ARGUMENT, "slot keys out of range or repeated");
+    }
+    return G4B_OK;
 }
 
 int g4b_eval_fresnel(int device, uint32_t precision, uint32_t n, const double* direction, const double* polarization,

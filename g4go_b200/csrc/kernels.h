@@ -37,6 +37,19 @@ cudaError_t LaunchOrderHits(const HitColumns& hits, unsigned long long count, st
                             std::uint32_t* bitmap, std::uint32_t* prefix, std::uint32_t* blockSums,
                             void* detectionsOut, bool ordered, cudaStream_t stream);
 
+// Ordering of caller-owned detection records by a unique slot key below
+// slotLimit (at most kStaticOrderMaxSlots) with all scratch in one array
+// compiled into the library. StaticOrderScratch gives that array's address on
+// the current device. LaunchOrderRecordsStatic enqueues the ranking on
+// `stream`, copies the count of rejected keys (out of range or repeated) to
+// *statusHost and waits for the stream. Calls that overlap in time on one
+// device share the array and race.
+constexpr std::uint32_t kStaticOrderMaxSlots{1U << 24};
+cudaError_t StaticOrderScratch(std::uint32_t** scratch);
+cudaError_t LaunchOrderRecordsStatic(const void* records, const std::uint32_t* keys, unsigned long long count,
+                                     std::uint32_t slotLimit, std::uint32_t* scratch, void* out,
+                                     std::uint32_t* statusHost, cudaStream_t stream);
+
 // Gradient replay over the `count` detected photons of the last transport:
 // each one is regenerated and re-transported from its RNG counters with dual
 // numbers, and its score and pathwise terms are summed into `sums`.

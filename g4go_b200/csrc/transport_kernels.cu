@@ -651,6 +651,65 @@ __global__ void ScatterDetections(const HitColumns hits, unsigned long long coun
     }
 }
 
+// --- ordering into a fixed scratch array ---------------------------------
+//
+// The same bitmap / block-sum / word-prefix ranking as above, for callers that
+// cannot allocate device memory: the three scratch arrays and a status word
+// live in one array compiled into the library, sized for kStaticOrderMaxSlots
+// slot keys (2 MiB bitmap + 2 MiB prefix + 2 KiB block sums).
+
+constexpr std::uint32_t kStaticOrderWords{kStaticOrderMaxSlots / 32U};
+constexpr std::uint32_t kStaticOrderBlocks{kStaticOrderWords / 1024U};
+constexpr std::uint32_t kStaticPrefixOffset{kStaticOrderWords};
+constexpr std::uint32_t kStaticSumsOffset{2U * kStaticOrderWords};
+constexpr std::uint32_t kStaticStatusOffset{kStaticSumsOffset + kStaticOrderBlocks + 64U};
+constexpr std::uint32_t kStaticScratchWords{kStaticStatusOffset + 64U};
+
+static __device__ __align__(256) std::uint32_t gStaticOrderScratch[kStaticScratchWords];
+
+// Marks each record's slot key in the bitmap. A key at or above slotLimit,
+// or one already marked, touches nothing and adds one to *status.
+__global__ void MarkKeysChecked(const std::uint32_t* __restrict__ keys, unsigned long long count,
+                                std::uint32_t slotLimit, std::uint32_t* __restrict__ bitmap,
+                                std::uint32_t* __restrict__ status) {
+    for (unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+        const std::uint32_t key{keys[i]};
+        if (key >= slotLimit) {
+            atomicAdd(status, 1U);
+            continue;
+        }
+        const std::uint32_t bit{1U << (key & 31U)};
+        if ((atomicOr(bitmap + (key >> 5U), bit) & bit) != 0U) {
+            atomicAdd(status, 1U);
+        }
+    }
+}
+
+// Copies each 48-byte record to the rank of its key among the marked keys.
+// Ranks stay below the number of marked keys, which is at most `count`, so
+// every store lands inside `out` even when keys were rejected above.
+__global__ void ScatterRecords(const float4* __restrict__ in, const std::uint32_t* __restrict__ keys,
+                               unsigned long long count, std::uint32_t slotLimit,
+                               const std::uint32_t* __restrict__ bitmap, const std::uint32_t* __restrict__ prefix,
+                               float4* __restrict__ out) {
+    for (unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+        const std::uint32_t key{keys[i]};
+        if (key >= slotLimit) {
+            continue;
+        }
+        const std::uint32_t word{key >> 5U};
+        const std::uint32_t below{bitmap[word] & ((1U << (key & 31U)) - 1U)};
+        const unsigned long long row{prefix[word] + static_cast<std::uint32_t>(__popc(below))};
+        const float4* source{in + i * 3ULL};
+        float4* target{out + row * 3ULL};
+        target[0] = source[0];
+        target[1] = source[1];
+        target[2] = source[2];
+    }
+}
+
 // --- device evaluation of single functions ------------------------------
 
 template<class R>
@@ -787,6 +846,44 @@ cudaError_t LaunchOrderHits(const HitColumns& hits, unsigned long long count, st
     ScatterDetections<<<BlocksFor(count, 256U), 256, 0, stream>>>(hits, count, bitmap, prefix, ordered,
                                                                   static_cast<float4*>(detectionsOut));
     return cudaGetLastError();
+}
+
+cudaError_t StaticOrderScratch(std::uint32_t** scratch) {
+    return cudaGetSymbolAddress(reinterpret_cast<void**>(scratch), gStaticOrderScratch);
+}
+
+cudaError_t LaunchOrderRecordsStatic(const void* records, const std::uint32_t* keys, unsigned long long count,
+                                     std::uint32_t slotLimit, std::uint32_t* scratch, void* out,
+                                     std::uint32_t* statusHost, cudaStream_t stream) {
+    std::uint32_t* bitmap{scratch};
+    std::uint32_t* prefix{scratch + kStaticPrefixOffset};
+    std::uint32_t* blockSums{scratch + kStaticSumsOffset};
+    std::uint32_t* status{scratch + kStaticStatusOffset};
+    const std::uint32_t words{(slotLimit + 31U) / 32U};
+    const std::uint32_t blocks{(words + 1023U) / 1024U};
+    // the bitmap and the status word must start at zero; prefix and block
+    // sums are fully rewritten below
+    cudaError_t error{cudaMemsetAsync(bitmap, 0, static_cast<std::size_t>(words) * 4U, stream)};
+    if (error == cudaSuccess) {
+        error = cudaMemsetAsync(status, 0, sizeof(std::uint32_t), stream);
+    }
+    if (error != cudaSuccess) {
+        return error;
+    }
+    MarkKeysChecked<<<BlocksFor(count, 256U), 256, 0, stream>>>(keys, count, slotLimit, bitmap, status);
+    BlockPopcount<<<blocks, 256, 0, stream>>>(bitmap, words, blockSums);
+    ScanBlockSums<<<1, 1024, 0, stream>>>(blockSums, blocks);
+    WordPrefix<<<blocks, 256, 0, stream>>>(bitmap, words, blockSums, prefix);
+    ScatterRecords<<<BlocksFor(count, 256U), 256, 0, stream>>>(static_cast<const float4*>(records), keys, count,
+                                                               slotLimit, bitmap, prefix, static_cast<float4*>(out));
+    error = cudaGetLastError();
+    if (error == cudaSuccess) {
+        error = cudaMemcpyAsync(statusHost, status, sizeof(std::uint32_t), cudaMemcpyDeviceToHost, stream);
+    }
+    if (error == cudaSuccess) {
+        error = cudaStreamSynchronize(stream);
+    }
+    return error;
 }
 
 cudaError_t LaunchGradientReplay(const LaunchParams& params, int precision, std::uint32_t indexMaterial,

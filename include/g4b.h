@@ -441,6 +441,37 @@ int g4b_eval_uniform(int device, uint32_t n, uint64_t seed, const uint64_t* phot
 int g4b_host_alloc(size_t bytes, void** pointer);
 int g4b_host_free(void* pointer);
 
+/* Orders device-resident detection records by a unique per-record slot key
+ * and allocates no device memory. No counterpart in the reference: it is the
+ * ranking step of the ordered completion (the order the reference's
+ * cub::DeviceSelect::Flagged compaction gives,
+ * src/optical/optix/OptiXHitCompaction.cu:23-30), offered on its own for
+ * callers that cannot allocate: a caller whose device memory is all held by
+ * its own pool, or one on a path where cudaMalloc/cudaFree would stall other
+ * streams by synchronizing the device.
+ *
+ * Record i of `unordered` is written to row r of `ordered`, r being the number
+ * of keys smaller than slots[i]; with the flattened photon index of a launch
+ * as key this restores the reference's order. All pointers are device
+ * memory on the current device, the record pointers 16-byte aligned, and
+ * `unordered` and `ordered` must not overlap. Keys must be unique and below
+ * slot_limit, and slot_limit at most G4B_ORDER_STATIC_MAX_SLOTS
+ * (G4B_ERR_OVERFLOW otherwise). A key out of range or repeated gives
+ * G4B_ERR_INVALID_ARGUMENT and leaves `ordered` undefined.
+ *
+ * Scratch is one 4 MiB array compiled into the library (bitmap, prefix and
+ * block sums); each call zeroes the bitmap and its status word on `stream`
+ * before use. The first call on a device looks the array up with
+ * cudaGetSymbolAddress, which may load the library's kernels there: make that
+ * call before any stream capture starts on the device. The first call on a
+ * host thread reserves a 256-byte host buffer for error messages; later calls
+ * allocate nothing. The call returns once `stream` has finished the
+ * ordering. Calls that overlap in time on one device share the scratch array
+ * and race: callers on several host threads must serialize them. */
+#define G4B_ORDER_STATIC_MAX_SLOTS 16777216u
+int g4b_order_detections_static(const g4b_photon_detection* unordered, const uint32_t* slots, uint64_t count,
+                                uint32_t slot_limit, g4b_photon_detection* ordered, void* stream);
+
 /* Version of this library (G4B_ABI_VERSION). */
 uint32_t g4b_abi_version(void);
 
