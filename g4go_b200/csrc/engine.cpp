@@ -218,12 +218,14 @@ std::size_t SceneSharedBytes(const g4b_handle& h) {
 }
 
 // Dynamic shared memory of a launch: the scene blob, plus one photon queue
-// per warp for the batched form.
+// and one Fresnel ring per warp for the batched form.
 std::size_t SharedBytes(const g4b_handle& h, int form, std::uint32_t blockSize) {
     std::size_t bytes{SceneSharedBytes(h)};
     if (form == g4b::kBatched) {
-        const std::size_t queue{h.config.precision == G4B_PRECISION_FP64 ? g4b::kQueueBytesFP64 : g4b::kQueueBytesFP32};
-        bytes += queue * (blockSize / 32U);
+        const bool fp64{h.config.precision == G4B_PRECISION_FP64};
+        const std::size_t queue{fp64 ? g4b::kQueueBytesFP64 : g4b::kQueueBytesFP32};
+        const std::size_t ring{fp64 ? g4b::kRingBytesFP64 : g4b::kRingBytesFP32};
+        bytes += (queue + ring) * (blockSize / 32U);
     }
     return bytes;
 }
@@ -536,7 +538,8 @@ void BuildScene(g4b_handle& h, const g4b_scene& scene) {
     }
     h.dScene.Ensure(blob.size(), "cudaMalloc scene");
     Check(cudaMemcpy(h.dScene.pointer, blob.data(), blob.size(), cudaMemcpyHostToDevice), "cudaMemcpy scene");
-    Check(g4b::ConfigureTransportKernels(((blob.size() + 15U) & ~std::size_t{15}) + 8U * g4b::kQueueBytesFP64),
+    Check(g4b::ConfigureTransportKernels(((blob.size() + 15U) & ~std::size_t{15}) +
+                                         8U * (g4b::kQueueBytesFP64 + g4b::kRingBytesFP64)),
           "cudaFuncSetAttribute shared memory");
     h.sceneBlob = std::move(blob);
     h.sceneBytes = static_cast<std::uint32_t>(h.sceneBlob.size());
@@ -1428,8 +1431,10 @@ int g4b_gradients(g4b_handle* h, const g4b_gradient_request* request, g4b_gradie
         Check(cudaMemsetAsync(h->dGradient.pointer, 0, sizeof(g4b::GradientSums), h->stream), "cudaMemsetAsync");
         const LaunchParams p{BaseParams(*h)};
         Check(cudaEventRecord(h->kernelTimer.start, h->stream), "cudaEventRecord");
+        // a grid-stride replay: a few resident 128-thread blocks per SM
+        const unsigned grid{static_cast<unsigned>(h->smCount) * 8U};
         Check(g4b::LaunchGradientReplay(p, Precision(*h), request->rindex_material_id, request->abs_length_material_id,
-                                        request->reflectivity_surface_id, hits, SceneSharedBytes(*h),
+                                        request->reflectivity_surface_id, grid, SceneSharedBytes(*h),
                                         h->dGradient.As<g4b::GradientSums>(), h->stream),
               "gradient replay");
         Check(cudaEventRecord(h->kernelTimer.stop, h->stream), "cudaEventRecord");
@@ -1438,10 +1443,10 @@ int g4b_gradients(g4b_handle* h, const g4b_gradient_request* request, g4b_gradie
         Check(cudaMemcpyAsync(&sums, h->dGradient.pointer, sizeof(sums), cudaMemcpyDeviceToHost, h->stream),
               "cudaMemcpyAsync gradient sums");
         Check(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
-        // N = sum 1; mean t = sum t / N; dN = sum S; d(mean t) = (sum (t S + dt) - mean t * sum S) / N.
+        // N = sum f; mean t = sum f t / N; dN = sum dN_i; d(mean t) = (d(sum f t) - mean t * dN) / N.
         g4b_gradient_result out{};
         out.detected = static_cast<std::uint64_t>(sums.detected);
-        out.replay_mismatches = sums.mismatches;
+        out.replay_mismatches = out.detected > hits ? out.detected - hits : hits - out.detected;
         const double n{sums.detected};
         out.mean_time_ns = n > 0.0 ? sums.time / n : 0.0;
         for (int j{}; j < 4; ++j) {

@@ -98,6 +98,11 @@ static_assert(sizeof(PackedScene) % 16 == 0, "scene blob must stay 16-byte align
 // transport type; time in double; eventID, photonID, volume, event index, slot.
 constexpr std::uint32_t kQueueBytesFP32 = 10U * 32U * 4U + 32U * 8U + 5U * 32U * 4U;  // 2176
 constexpr std::uint32_t kQueueBytesFP64 = 10U * 32U * 8U + 32U * 8U + 5U * 32U * 4U;  // 3456
+// Per-warp ring of photons stopped at a Fresnel boundary (pending) or done
+// with it (ready): 12 real columns, FP64 time, 7 u32 columns, 64 entries.
+constexpr std::uint32_t kFresnelRingEntries = 64;
+constexpr std::uint32_t kRingBytesFP32 = kFresnelRingEntries * (12U * 4U + 8U + 7U * 4U);  // 5376
+constexpr std::uint32_t kRingBytesFP64 = kFresnelRingEntries * (12U * 8U + 8U + 7U * 4U);  // 8448
 
 // Per-event counters (DeviceEventTransportStats, OptiXDeviceData.cuh:159-167),
 // padded to 64 bytes.
@@ -130,7 +135,7 @@ struct GradientSums {
     double time;           // sum of arrival times
     double score[4];       // sum of S_j (score + pathwise log-probability terms)
     double timeScore[4];   // sum of t S_j + dt/dtheta_j
-    unsigned long long mismatches;  // detected photons the replay did not reproduce
+    unsigned long long mismatches;  // unused (the host compares detected counts)
     unsigned long long reserved;
 };
 

@@ -82,11 +82,6 @@ __device__ __forceinline__ Dual<T> Sqrt(Dual<T> a) {
     return MakeDual(r, a.d == T(0) ? T(0) : a.d / (T(2) * r));
 }
 template<class T>
-__device__ __forceinline__ Dual<T> Rsqrt(Dual<T> a) {
-    const T r{Rsqrt(a.v)};
-    return MakeDual(r, T(-0.5) * a.d * r * r * r);
-}
-template<class T>
 __device__ __forceinline__ Dual<T> Fabs(Dual<T> a) { return a.v < T(0) ? -a : a; }
 template<class T>
 __device__ __forceinline__ Dual<T> Fmin(Dual<T> a, Dual<T> b) {

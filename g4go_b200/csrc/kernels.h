@@ -50,13 +50,13 @@ cudaError_t LaunchOrderRecordsStatic(const void* records, const std::uint32_t* k
                                      std::uint32_t slotLimit, std::uint32_t* scratch, void* out,
                                      std::uint32_t* statusHost, cudaStream_t stream);
 
-// Gradient replay over the `count` detected photons of the last transport:
-// each one is regenerated and re-transported from its RNG counters with dual
-// numbers, and its score and pathwise terms are summed into `sums`.
+// Gradient replay over the photons [photonBegin, photonEnd) of the last
+// transport: each one is regenerated and re-transported from its RNG counters
+// with dual numbers, alternate branches of its Fresnel choices transported
+// when an index target is set, and its derivative terms summed into `sums`.
 cudaError_t LaunchGradientReplay(const LaunchParams& params, int precision, std::uint32_t indexMaterial,
-                                 std::uint32_t absMaterial, std::uint32_t reflectivitySurface,
-                                 unsigned long long count, std::size_t sharedBytes, GradientSums* sums,
-                                 cudaStream_t stream);
+                                 std::uint32_t absMaterial, std::uint32_t reflectivitySurface, unsigned grid,
+                                 std::size_t sharedBytes, GradientSums* sums, cudaStream_t stream);
 
 cudaError_t LaunchEvalFresnel(int precision, std::uint32_t n, const double* in, double* out, cudaStream_t stream);
 cudaError_t LaunchEvalLambertian(int precision, std::uint32_t n, const double* in, double* out, cudaStream_t stream);

@@ -218,6 +218,117 @@ struct WarpQueue {
 static_assert(sizeof(WarpQueue<float>) == kQueueBytesFP32, "queue layout");
 static_assert(sizeof(WarpQueue<double>) == kQueueBytesFP64, "queue layout");
 
+// The shared-memory Fresnel ring of one warp. Steps that stop at a boundary
+// without a surface park here as pending jobs; once 32 are pending the whole
+// warp completes them together (one job per lane) and they stay in place as
+// ready photons, which idle lanes take before fresh ones. Entries are used in
+// ring order: [readyHead, pendingHead) ready, [pendingHead, pendingEnd) pending.
+template<class R>
+struct FresnelRing {
+    static constexpr std::uint32_t kEntries = kFresnelRingEntries;
+    R positionX[kEntries], positionY[kEntries], positionZ[kEntries];  // the boundary point while pending
+    R directionX[kEntries], directionY[kEntries], directionZ[kEntries];
+    R polarizationX[kEntries], polarizationY[kEntries], polarizationZ[kEntries];
+    R energy[kEntries], indexFrom[kEntries], indexTo[kEntries];
+    double time[kEntries];
+    std::uint32_t eventID[kEntries], photonID[kEntries], volume[kEntries], eventIndex[kEntries], slot[kEntries],
+        bounce[kEntries];
+    // pending: next volume | normal axis << 8 | sign bits of the normal << 10; ready: the step result
+    std::uint32_t link[kEntries];
+
+    __device__ __forceinline__ void PutPhoton(unsigned k, const Photon<R>& photon) {
+        directionX[k] = photon.direction.x;
+        directionY[k] = photon.direction.y;
+        directionZ[k] = photon.direction.z;
+        polarizationX[k] = photon.polarization.x;
+        polarizationY[k] = photon.polarization.y;
+        polarizationZ[k] = photon.polarization.z;
+        energy[k] = photon.energy;
+        time[k] = photon.time;
+        eventID[k] = photon.eventID;
+        photonID[k] = photon.photonID;
+        volume[k] = photon.volume;
+        eventIndex[k] = photon.eventIndex;
+        slot[k] = photon.slot;
+        bounce[k] = photon.bounce;
+    }
+    __device__ __forceinline__ void TakePhoton(unsigned k, Photon<R>& photon) const {
+        photon.position = {positionX[k], positionY[k], positionZ[k]};
+        photon.direction = {directionX[k], directionY[k], directionZ[k]};
+        photon.polarization = {polarizationX[k], polarizationY[k], polarizationZ[k]};
+        photon.energy = energy[k];
+        photon.time = time[k];
+        photon.eventID = eventID[k];
+        photon.photonID = photonID[k];
+        photon.volume = volume[k];
+        photon.eventIndex = eventIndex[k];
+        photon.slot = slot[k];
+        photon.bounce = bounce[k];
+    }
+    __device__ __forceinline__ void PutJob(unsigned k, const Photon<R>& photon, const FresnelJob<R>& job) {
+        PutPhoton(k, photon);
+        positionX[k] = job.boundary.x;
+        positionY[k] = job.boundary.y;
+        positionZ[k] = job.boundary.z;
+        indexFrom[k] = job.indexFrom;
+        indexTo[k] = job.indexTo;
+        // the boundary normal is a unit axis of a box face; the signs of all
+        // three components are kept, zeros included, so the completed step
+        // is bit-identical to one finished in place
+        const std::uint32_t axis{job.normal.x != R(0) ? 0U : (job.normal.y != R(0) ? 1U : 2U)};
+        link[k] = job.next | (axis << 8U) | (static_cast<std::uint32_t>(signbit(job.normal.x)) << 10U) |
+                  (static_cast<std::uint32_t>(signbit(job.normal.y)) << 11U) |
+                  (static_cast<std::uint32_t>(signbit(job.normal.z)) << 12U);
+    }
+    __device__ __forceinline__ void TakeJob(unsigned k, Photon<R>& photon, FresnelJob<R>& job) const {
+        TakePhoton(k, photon);
+        job.boundary = photon.position;
+        job.indexFrom = indexFrom[k];
+        job.indexTo = indexTo[k];
+        const std::uint32_t code{link[k]};
+        job.next = code & 0xffU;
+        const std::uint32_t axis{(code >> 8U) & 3U};
+        const R x{axis == 0U ? R(1) : R(0)}, y{axis == 1U ? R(1) : R(0)}, z{axis == 2U ? R(1) : R(0)};
+        job.normal = {((code >> 10U) & 1U) != 0U ? -x : x, ((code >> 11U) & 1U) != 0U ? -y : y,
+                      ((code >> 12U) & 1U) != 0U ? -z : z};
+    }
+    __device__ __forceinline__ void PutReady(unsigned k, const Photon<R>& photon, std::uint32_t result) {
+        PutPhoton(k, photon);
+        positionX[k] = photon.position.x;
+        positionY[k] = photon.position.y;
+        positionZ[k] = photon.position.z;
+        link[k] = result;
+    }
+};
+static_assert(sizeof(FresnelRing<float>) == kRingBytesFP32, "ring layout");
+static_assert(sizeof(FresnelRing<double>) == kRingBytesFP64, "ring layout");
+
+// A Fresnel step completed in the lane that reached it, when the ring is full.
+template<class R>
+G4B_COLD std::uint32_t FinishFresnelHere(Photon<R>& photon, const FresnelJob<R>& job, unsigned long long seed,
+                                         std::uint32_t maxBounce, R epsilon) {
+    return FinishFresnel(photon, job.boundary, job.normal, job.indexFrom, job.indexTo, job.next, seed, maxBounce,
+                         epsilon);
+}
+
+// Completes `count` (<= 32) pending Fresnel jobs from pendingHead, one per
+// lane, leaving them in place as ready photons.
+template<class R>
+__device__ __forceinline__ void ResolvePending(FresnelRing<R>& ring, std::uint32_t& pendingHead, std::uint32_t count,
+                                               unsigned lane, const LaunchParams& p, R epsilon) {
+    if (lane < count) {
+        const unsigned k{(pendingHead + lane) % FresnelRing<R>::kEntries};
+        Photon<R> photon{};
+        FresnelJob<R> job;
+        ring.TakeJob(k, photon, job);
+        const std::uint32_t result{FinishFresnel(photon, job.boundary, job.normal, job.indexFrom, job.indexTo, job.next,
+                                                 p.seed, p.maxBounce, epsilon)};
+        ring.PutReady(k, photon, result);
+    }
+    pendingHead += count;
+    __syncwarp();
+}
+
 // Persistent transport. Each warp owns a 32-entry photon queue in shared
 // memory. When the queue is empty and a lane needs a photon, the whole warp
 // takes the next 32 flattened photon indices of its chunk (one atomic on the
@@ -245,8 +356,15 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
     const unsigned lanesBelow{(1U << lane) - 1U};
     const R epsilon{R(p.epsilon)};
     const std::uint32_t totalPhotons{p.photonEnd - p.photonBegin};
-    WarpQueue<R>& queue{*reinterpret_cast<WarpQueue<R>*>(gShared + ((p.sceneBytes + 15U) & ~15U) +
-                                                         (threadIdx.x >> 5U) * sizeof(WarpQueue<R>))};
+    const std::uint32_t sceneEnd{(p.sceneBytes + 15U) & ~15U};
+    WarpQueue<R>& queue{
+        *reinterpret_cast<WarpQueue<R>*>(gShared + sceneEnd + (threadIdx.x >> 5U) * sizeof(WarpQueue<R>))};
+    FresnelRing<R>& ring{*reinterpret_cast<FresnelRing<R>*>(gShared + sceneEnd + (blockDim.x >> 5U) * sizeof(WarpQueue<R>) +
+                                                            (threadIdx.x >> 5U) * sizeof(FresnelRing<R>))};
+    constexpr std::uint32_t kRing{FresnelRing<R>::kEntries};
+    std::uint32_t readyHead{0U};
+    std::uint32_t pendingHead{0U};
+    std::uint32_t pendingEnd{0U};
 
     std::uint32_t chunkNext{0U};
     std::uint32_t chunkEnd{0U};
@@ -265,6 +383,27 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
 
     for (;;) {
         unsigned need{__ballot_sync(kFullMask, !alive)};
+        // Photons done with their Fresnel boundary go first.
+        if (need != 0U && pendingHead != readyHead) {
+            const std::uint32_t ready{pendingHead - readyHead};
+            const std::uint32_t rank{static_cast<std::uint32_t>(__popc(need & lanesBelow))};
+            if (!alive && rank < ready) {
+                const unsigned k{(readyHead + rank) % kRing};
+                ring.TakePhoton(k, photon);
+                const std::uint32_t status{ring.link[k]};
+                counters.Switch(photon.eventIndex, p.events);
+                if (status == kContinue) {
+                    alive = true;
+                } else {  // truncated by the Fresnel step's bounce
+                    counters.Finish(status, photon.bounce);
+                    laneBounces += photon.bounce;
+                    RecordFate(p, photon.slot, status, photon.bounce, photon.time);
+                }
+            }
+            readyHead += min(static_cast<std::uint32_t>(__popc(need)), ready);
+            __syncwarp();
+            need = __ballot_sync(kFullMask, !alive);
+        }
         while (need != 0U) {
             if (queueHead == queueCount) {
                 if (workDone) {
@@ -332,20 +471,45 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
             need = __ballot_sync(kFullMask, !alive);
         }
         if (__ballot_sync(kFullMask, alive) == 0U) {
+            if (pendingEnd != pendingHead) {
+                // no fresh work left: complete what is pending, even if fewer than 32
+                ResolvePending(ring, pendingHead, min(pendingEnd - pendingHead, 32U), lane, p, epsilon);
+                continue;
+            }
+            if (pendingHead != readyHead) {
+                continue;
+            }
             break;
         }
 
         std::uint32_t result{kContinue};
         StepExtras extras{0U, 0U, 0U, 0U};
+        FresnelJob<R> job;
         if (alive) {
-            result = StepPhoton<R>(scene, pool, photon, p.seed, p.maxBounce, epsilon, extras, NoGradient());
+            result = StepPhoton<R, true>(scene, pool, photon, p.seed, p.maxBounce, epsilon, extras, NoGradient(), &job);
+        }
+        const bool parking{alive && result == kFresnelPending};
+        const unsigned parkMask{__ballot_sync(kFullMask, parking)};
+        if (parkMask != 0U) {
+            const std::uint32_t room{kRing - (pendingEnd - readyHead)};
+            if (parking) {
+                const std::uint32_t rank{static_cast<std::uint32_t>(__popc(parkMask & lanesBelow))};
+                if (rank < room) {
+                    ring.PutJob((pendingEnd + rank) % kRing, photon, job);
+                } else {
+                    result = FinishFresnelHere(photon, job, p.seed, p.maxBounce, epsilon);
+                }
+            }
+            pendingEnd += min(static_cast<std::uint32_t>(__popc(parkMask)), room);
         }
         WriteHits(alive && result == kDetected, photon, extras.sensorID, p, lane);
         if (alive) {
             counters.zeroStep += extras.zeroSteps;
             coincidentTraces += extras.coincidentTraces;
             coincidentHits += extras.coincidentHits;
-            if (result != kContinue) {
+            if (result == kFresnelPending) {
+                alive = false;
+            } else if (result != kContinue) {
                 const std::uint32_t bounces{result == kTruncated ? photon.bounce : photon.bounce + 1U};
                 counters.Finish(result, bounces);
                 laneBounces += bounces;
@@ -354,6 +518,9 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
             }
         }
         __syncwarp();
+        if (pendingEnd - pendingHead >= 32U) {
+            ResolvePending(ring, pendingHead, 32U, lane, p, epsilon);
+        }
     }
     counters.Flush(p.events);
     FlushRunCounters(p, laneBounces, coincidentTraces, coincidentHits, lane);
@@ -416,57 +583,110 @@ __global__ void __launch_bounds__(256) TransportPlain(const LaunchParams p) {
     FlushRunCounters(p, laneBounces, coincidentTraces, coincidentHits, lane);
 }
 
-// Gradient replay: one thread per detected photon. The photon is regenerated
-// from its genstep and RNG counters and transported again with Dual<R>, which
-// repeats the forward history exactly (same values, same choices) while
-// carrying d/dn; the score terms of every discrete choice accumulate along the
-// way. Per-photon results are reduced per warp in FP64 and added to `sums`.
+// Seed of the draws of an alternate branch spawned at the step that ended
+// with bounce number `bounce`: independent of the photon's own draws.
+__device__ __forceinline__ unsigned long long AlternateSeed(unsigned long long seed, std::uint32_t bounce) {
+    return seed ^ (0x9E3779B97F4A7C15ULL * (static_cast<unsigned long long>(bounce) + 1ULL));
+}
+
+// Transports the branch a replayed photon did not take at its last Fresnel
+// choice to its end in plain arithmetic. Returns whether it was detected and
+// its arrival time.
+template<class R>
+__device__ bool RunAlternate(const PackedScene& scene, const float* pool, const LaunchParams& p,
+                             const Photon<Dual<R>>& taken, double* time) {
+    Photon<R> branch{};
+    branch.position = taken.tangents.alternatePosition;
+    branch.direction = taken.tangents.alternateDirection;
+    branch.polarization = taken.tangents.alternatePolarization;
+    branch.volume = taken.tangents.alternateVolume;
+    branch.time = taken.time;
+    branch.energy = taken.energy.v;
+    branch.bounce = taken.bounce;
+    branch.eventID = taken.eventID;
+    branch.photonID = taken.photonID;
+    if (branch.bounce >= p.maxBounce) {
+        return false;
+    }
+    const unsigned long long seed{AlternateSeed(p.seed, taken.bounce)};
+    const R epsilon{R(p.epsilon)};
+    StepExtras extras{0U, 0U, 0U, 0U};
+    std::uint32_t result;
+    do {
+        result = StepPhoton<R>(scene, pool, branch, seed, p.maxBounce, epsilon, extras, NoGradient());
+    } while (result == kContinue);
+    *time = branch.time;
+    return result == kDetected;
+}
+
+// Gradient replay: every photon of the batch is regenerated from its RNG
+// counters and re-transported with dual numbers (pathwise derivatives), its
+// score terms accumulating; with a refractive-index target each Fresnel choice
+// at a boundary without a surface spawns its alternate branch instead of a
+// score (measure-valued derivative, bounded where the score dT/T is not).
+// Per photon, with f its detection and t its arrival time:
+//   dN     += f (S + W) - sum_k w_k f_k
+//   d(tN)  += f (t (S + W) + dt) - sum_k w_k f_k t_k
+// where S is the score, w_k = +-dT/dn of choice k, W = sum w_k and f_k, t_k the
+// outcome of its alternate. Grid-stride over the photons, FP64 sums reduced
+// per warp at the end.
 template<class R>
 __global__ void __launch_bounds__(128) GradientReplay(const LaunchParams p, GradientTargets targets,
-                                                      unsigned long long count, GradientSums* sums) {
+                                                      GradientSums* sums) {
     using D = Dual<R>;
     LoadScene(p);
     const PackedScene& scene{*reinterpret_cast<const PackedScene*>(gShared)};
     const float* pool{PoolOf(scene)};
-    const unsigned long long i{blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x};
-    double values[11]{};
-    if (i < count) {
-        const std::uint32_t slot{p.hits.slot[i]};
+    double values[10]{};
+    for (std::uint32_t slot = p.photonBegin + blockIdx.x * blockDim.x + threadIdx.x; slot < p.photonEnd;
+         slot += gridDim.x * blockDim.x) {
         const std::uint32_t e{FindEmission(p.emissionOffsets, 0U, p.emissionCount, slot)};
         Emission emission;
         LoadEmission(p.emissions, e, emission);
         const std::uint32_t local{slot - __ldg(p.emissionOffsets + e)};
         Photon<D> photon{};
+        photon.tangents.alternates = targets.indexMaterial != kInvalidID;
         GeneratePhoton<D>(scene, pool, emission, emission.FirstPhotonID() + local, p.seed, targets, photon);
         photon.slot = slot;
         std::uint32_t result{kInvalid};
         StepExtras extras{0U, 0U, 0U, 0U};
+        double weights{0.0};
+        double alternateDetected{0.0};
+        double alternateTime{0.0};
         if (StartPhoton(photon)) {
             const D epsilon{p.epsilon};
             do {
                 result = StepPhoton<D>(scene, pool, photon, p.seed, p.maxBounce, epsilon, extras, targets);
+                if (photon.tangents.alternatePending) {
+                    photon.tangents.alternatePending = false;
+                    const double w{photon.tangents.alternateWeight};
+                    double time{0.0};
+                    weights += w;
+                    if (RunAlternate(scene, pool, p, photon, &time)) {
+                        alternateDetected += w;
+                        alternateTime += w * time;
+                    }
+                }
             } while (result == kContinue);
         }
-        const bool reproduced{result == kDetected && extras.sensorID == p.hits.sensorID[i] &&
-                              static_cast<float>(photon.time) == p.hits.time[i]};
-        if (reproduced) {
+        values[2] -= alternateDetected;
+        values[6] -= alternateTime;
+        if (result == kDetected) {
             const double t{photon.time};
-            const double score[4]{photon.tangents.scoreIndex, photon.tangents.scoreAbsLength,
+            const double score[4]{photon.tangents.scoreIndex + weights, photon.tangents.scoreAbsLength,
                                   photon.tangents.scoreReflectivity, 0.0};
             const double dt[4]{photon.tangents.dTimeDIndex, 0.0, 0.0, photon.tangents.dTimeDDecay};
-            values[0] = 1.0;
-            values[1] = t;
+            values[0] += 1.0;
+            values[1] += t;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                values[2 + j] = score[j];
-                values[6 + j] = t * score[j] + dt[j];
+                values[2 + j] += score[j];
+                values[6 + j] += t * score[j] + dt[j];
             }
-        } else {
-            values[10] = 1.0;
         }
     }
 #pragma unroll
-    for (int k = 0; k < 11; ++k) {
+    for (int k = 0; k < 10; ++k) {
 #pragma unroll
         for (int offset = 16; offset > 0; offset >>= 1) {
             values[k] += __shfl_down_sync(kFullMask, values[k], offset);
@@ -479,9 +699,6 @@ __global__ void __launch_bounds__(128) GradientReplay(const LaunchParams p, Grad
         for (int j = 0; j < 4; ++j) {
             atomicAdd(&sums->score[j], values[2 + j]);
             atomicAdd(&sums->timeScore[j], values[6 + j]);
-        }
-        if (values[10] != 0.0) {
-            atomicAdd(&sums->mismatches, static_cast<unsigned long long>(values[10]));
         }
     }
 }
@@ -887,9 +1104,8 @@ cudaError_t LaunchOrderRecordsStatic(const void* records, const std::uint32_t* k
 }
 
 cudaError_t LaunchGradientReplay(const LaunchParams& params, int precision, std::uint32_t indexMaterial,
-                                 std::uint32_t absMaterial, std::uint32_t reflectivitySurface,
-                                 unsigned long long count, std::size_t sharedBytes, GradientSums* sums,
-                                 cudaStream_t stream) {
+                                 std::uint32_t absMaterial, std::uint32_t reflectivitySurface, unsigned grid,
+                                 std::size_t sharedBytes, GradientSums* sums, cudaStream_t stream) {
     const GradientTargets targets{indexMaterial, absMaterial, reflectivitySurface};
     const void* kernel{precision == kFP64 ? reinterpret_cast<const void*>(&GradientReplay<double>)
                                           : reinterpret_cast<const void*>(&GradientReplay<float>)};
@@ -898,14 +1114,13 @@ cudaError_t LaunchGradientReplay(const LaunchParams& params, int precision, std:
     if (error != cudaSuccess) {
         return error;
     }
-    if (count == 0ULL) {
+    if (params.photonEnd <= params.photonBegin) {
         return cudaSuccess;
     }
-    const unsigned blocks{static_cast<unsigned>((count + 127ULL) / 128ULL)};
     if (precision == kFP64) {
-        GradientReplay<double><<<blocks, 128, sharedBytes, stream>>>(params, targets, count, sums);
+        GradientReplay<double><<<grid, 128, sharedBytes, stream>>>(params, targets, sums);
     } else {
-        GradientReplay<float><<<blocks, 128, sharedBytes, stream>>>(params, targets, count, sums);
+        GradientReplay<float><<<grid, 128, sharedBytes, stream>>>(params, targets, sums);
     }
     return cudaGetLastError();
 }

@@ -378,15 +378,19 @@ int g4b_autotune(g4b_handle* handle, const uint32_t* block_sizes, uint32_t n_blo
  * completed on this handle (same gensteps, same seed): a refractive index
  * (of one material, constant RINDEX table), an absorption length (one
  * material), a reflectivity (one surface) and the scintillation decay time
- * (all scintillation gensteps). Each detected photon is regenerated and
+ * (all scintillation gensteps). Every photon of the batch is regenerated and
  * re-transported from its RNG counters with forward-mode dual numbers
  * (pathwise derivatives through the step loop) while the score terms
- * d log p / d theta of its discrete choices (Fresnel reflect/transmit,
- * surface classification, survival of bulk absorption) accumulate; nothing
- * of the forward trajectories is stored. FP32 replay for an FP32 handle with
- * FP64 accumulation. Geometric discontinuities (a changed parameter moving a
- * photon to another face) are not included. Batches the plain form regrouped
- * by event are not supported. */
+ * d log p / d theta of its discrete choices (surface classification, survival
+ * of bulk absorption, Fresnel choices at surfaces) accumulate. For the
+ * refractive index, a Fresnel choice at a boundary without a surface uses the
+ * measure-valued form instead of a score: the branch not taken is transported
+ * to its end with draws of its own, and the difference of the two outcomes is
+ * weighted by dT/dn (the score dT/T has unbounded variance near the critical
+ * angle). Nothing of the forward trajectories is stored. FP32 replay for an
+ * FP32 handle with FP64 accumulation. Geometric discontinuities (a changed
+ * parameter moving a photon across the edge of a face) are not included.
+ * Batches the plain form regrouped by event are not supported. */
 typedef struct g4b_gradient_request {
     uint32_t rindex_material_id;      /* G4B_INVALID_ID: no index derivative */
     uint32_t abs_length_material_id;  /* G4B_INVALID_ID: none */
@@ -398,7 +402,7 @@ typedef struct g4b_gradient_request {
  * (per mm), 2 reflectivity, 3 scintillation decay time (per ns). */
 typedef struct g4b_gradient_result {
     uint64_t detected;
-    uint64_t replay_mismatches; /* detected photons the replay did not reproduce; 0 expected */
+    uint64_t replay_mismatches; /* |replayed detections - the batch's detections|; 0 expected */
     double mean_time_ns;
     double d_detected[4];
     double d_mean_time_ns[4];
