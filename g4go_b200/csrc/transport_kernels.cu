@@ -303,6 +303,7 @@ struct FresnelRing {
 static_assert(sizeof(FresnelRing<float>) == kRingBytesFP32, "ring layout");
 static_assert(sizeof(FresnelRing<double>) == kRingBytesFP64, "ring layout");
 
+
 // A Fresnel step completed in the lane that reached it, when the ring is full.
 template<class R>
 G4B_COLD std::uint32_t FinishFresnelHere(Photon<R>& photon, const FresnelJob<R>& job, unsigned long long seed,
