@@ -402,6 +402,13 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
                 }
             }
             readyHead += min(static_cast<std::uint32_t>(__popc(need)), ready);
+            if (readyHead >= kRing) {
+                // keep the three positions small; subtracting the ring size
+                // leaves every entry index (position mod kRing) unchanged
+                readyHead -= kRing;
+                pendingHead -= kRing;
+                pendingEnd -= kRing;
+            }
             __syncwarp();
             need = __ballot_sync(kFullMask, !alive);
         }
