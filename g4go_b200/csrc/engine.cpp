@@ -213,6 +213,12 @@ namespace {
 int Precision(const g4b_handle& h) { return h.config.precision == G4B_PRECISION_FP64 ? g4b::kFP64 : g4b::kFP32; }
 int Form(const g4b_handle& h) { return h.config.launch_form == G4B_FORM_PLAIN ? g4b::kPlain : g4b::kBatched; }
 
+// The kernel variant of a form: with the coincidence counters only when
+// performance diagnostics are enabled, as the reference counts them.
+int KernelOf(const g4b_handle& h, int form) {
+    return form | (h.config.enable_performance_diagnostics != 0 ? g4b::kWithDiagnostics : 0);
+}
+
 std::size_t SceneSharedBytes(const g4b_handle& h) {
     return (static_cast<std::size_t>(h.sceneBytes) + 15U) & ~std::size_t{15};
 }
@@ -613,7 +619,7 @@ void EnsureHitCapacity(g4b_handle& h, std::uint64_t rows) {
 unsigned BatchedGrid(g4b_handle& h) {
     if (h.blocksPerSM == 0) {
         int blocks{0};
-        Check(g4b::TransportOccupancy(Precision(h), g4b::kBatched, static_cast<int>(h.blockSize),
+        Check(g4b::TransportOccupancy(Precision(h), KernelOf(h, g4b::kBatched), static_cast<int>(h.blockSize),
                                       SharedBytes(h, g4b::kBatched, h.blockSize), &blocks),
               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
         h.blocksPerSM = static_cast<std::uint32_t>(std::max(blocks, 1));
@@ -650,7 +656,7 @@ void LaunchBatchedGraph(g4b_handle& h, const LaunchParams& params, unsigned grid
     zero.sharedMemBytes = 0;
     zero.kernelParams = zeroArgs;
     cudaKernelNodeParams transport{};
-    transport.func = const_cast<void*>(g4b::TransportKernel(Precision(h), g4b::kBatched));
+    transport.func = const_cast<void*>(g4b::TransportKernel(Precision(h), KernelOf(h, g4b::kBatched)));
     transport.gridDim = dim3(grid);
     transport.blockDim = dim3(h.blockSize);
     transport.sharedMemBytes = static_cast<unsigned>(SharedBytes(h, g4b::kBatched, h.blockSize));
@@ -691,7 +697,7 @@ void RunStaged(g4b_handle& h) {
             LaunchBatchedGraph(h, base, grid);
         } else {
             Check(g4b::LaunchZeroCounters(base.events, base.eventCount, base.run, h.stream), "zero counters");
-            Check(g4b::LaunchTransport(base, Precision(h), g4b::kBatched, grid, h.blockSize,
+            Check(g4b::LaunchTransport(base, Precision(h), KernelOf(h, g4b::kBatched), grid, h.blockSize,
                                        SharedBytes(h, g4b::kBatched, h.blockSize), h.stream),
                   "transport launch");
         }
@@ -707,7 +713,7 @@ void RunStaged(g4b_handle& h) {
             p.photonEnd = event.photonEnd;
             const std::uint32_t photons{event.photonEnd - event.photonBegin};
             const unsigned grid{(photons + h.blockSize - 1U) / h.blockSize};
-            Check(g4b::LaunchTransport(p, Precision(h), g4b::kPlain, grid, h.blockSize,
+            Check(g4b::LaunchTransport(p, Precision(h), KernelOf(h, g4b::kPlain), grid, h.blockSize,
                                        SharedBytes(h, g4b::kPlain, h.blockSize), h.stream),
                   "transport launch");
             ++h.launchCount;
@@ -1347,7 +1353,7 @@ int g4b_autotune(g4b_handle* h, const uint32_t* blockSizes, uint32_t nBlockSizes
                 Throw(G4B_ERR_INVALID_ARGUMENT, "autotune block sizes must be multiples of 32 up to 256");
             }
             int maxBlocks{0};
-            Check(g4b::TransportOccupancy(Precision(*h), g4b::kBatched, static_cast<int>(block),
+            Check(g4b::TransportOccupancy(Precision(*h), KernelOf(*h, g4b::kBatched), static_cast<int>(block),
                                           SharedBytes(*h, g4b::kBatched, block), &maxBlocks),
                   "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
             maxBlocks = std::max(maxBlocks, 1);
@@ -1370,7 +1376,7 @@ int g4b_autotune(g4b_handle* h, const uint32_t* blockSizes, uint32_t nBlockSizes
                     for (std::uint32_t r{}; r < repeats + 1; ++r) {
                         Check(g4b::LaunchZeroCounters(p.events, p.eventCount, p.run, h->stream), "zero counters");
                         Check(cudaEventRecord(h->kernelTimer.start, h->stream), "cudaEventRecord");
-                        Check(g4b::LaunchTransport(p, Precision(*h), g4b::kBatched, grid, block,
+                        Check(g4b::LaunchTransport(p, Precision(*h), KernelOf(*h, g4b::kBatched), grid, block,
                                                    SharedBytes(*h, g4b::kBatched, block), h->stream),
                               "transport launch");
                         Check(cudaEventRecord(h->kernelTimer.stop, h->stream), "cudaEventRecord");

@@ -11,10 +11,11 @@
 namespace g4b {
 
 enum KernelPrecision : int { kFP32 = 0, kFP64 = 1 };
-enum KernelForm : int { kBatched = 0, kPlain = 1 };
+enum KernelForm : int { kBatched = 0, kPlain = 1, kWithDiagnostics = 2 };
 
 // The transport kernel for (precision, form), as a function pointer usable in
-// cudaLaunchKernel and in graph kernel nodes.
+// cudaLaunchKernel and in graph kernel nodes. `form` may carry
+// kWithDiagnostics: the variant that also counts coincident-face retraces.
 const void* TransportKernel(int precision, int form);
 const void* ZeroCountersKernel();
 

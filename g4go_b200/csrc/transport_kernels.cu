@@ -348,7 +348,10 @@ struct BatchedMinBlocks<double> {
     static constexpr int value = 1;
 };
 
-template<class R>
+// kDiagnostics: count coincident-face retraces and hits, which the reference
+// does only with enablePerformanceDiagnostics (OptiXTransportDevice.cu:752-775);
+// without it the counting is compiled out, which frees registers in the loop.
+template<class R, bool kDiagnostics>
 __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatched(const LaunchParams p) {
     LoadScene(p);
     const PackedScene& scene{*reinterpret_cast<const PackedScene*>(gShared)};
@@ -513,8 +516,10 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
         WriteHits(alive && result == kDetected, photon, extras.sensorID, p, lane);
         if (alive) {
             counters.zeroStep += extras.zeroSteps;
-            coincidentTraces += extras.coincidentTraces;
-            coincidentHits += extras.coincidentHits;
+            if constexpr (kDiagnostics) {
+                coincidentTraces += extras.coincidentTraces;
+                coincidentHits += extras.coincidentHits;
+            }
             if (result == kFresnelPending) {
                 alive = false;
             } else if (result != kContinue) {
@@ -534,7 +539,7 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
     FlushRunCounters(p, laneBounces, coincidentTraces, coincidentHits, lane);
 }
 
-template<class R>
+template<class R, bool kDiagnostics>
 __global__ void __launch_bounds__(256) TransportPlain(const LaunchParams p) {
     LoadScene(p);
     const PackedScene& scene{*reinterpret_cast<const PackedScene*>(gShared)};
@@ -576,8 +581,10 @@ __global__ void __launch_bounds__(256) TransportPlain(const LaunchParams p) {
         WriteHits(alive && result == kDetected, photon, extras.sensorID, p, lane);
         if (alive) {
             counters.zeroStep += extras.zeroSteps;
-            coincidentTraces += extras.coincidentTraces;
-            coincidentHits += extras.coincidentHits;
+            if constexpr (kDiagnostics) {
+                coincidentTraces += extras.coincidentTraces;
+                coincidentHits += extras.coincidentHits;
+            }
             if (result != kContinue) {
                 const std::uint32_t bounces{result == kTruncated ? photon.bounce : photon.bounce + 1U};
                 counters.Finish(result, bounces);
@@ -1007,19 +1014,28 @@ unsigned BlocksFor(unsigned long long n, unsigned block) {
 }  // namespace
 
 const void* TransportKernel(int precision, int form) {
-    if (form == kPlain) {
-        return precision == kFP64 ? reinterpret_cast<const void*>(&TransportPlain<double>)
-                                  : reinterpret_cast<const void*>(&TransportPlain<float>);
+    const bool diagnostics{(form & kWithDiagnostics) != 0};
+    if ((form & ~kWithDiagnostics) == kPlain) {
+        if (precision == kFP64) {
+            return diagnostics ? reinterpret_cast<const void*>(&TransportPlain<double, true>)
+                               : reinterpret_cast<const void*>(&TransportPlain<double, false>);
+        }
+        return diagnostics ? reinterpret_cast<const void*>(&TransportPlain<float, true>)
+                           : reinterpret_cast<const void*>(&TransportPlain<float, false>);
     }
-    return precision == kFP64 ? reinterpret_cast<const void*>(&TransportBatched<double>)
-                              : reinterpret_cast<const void*>(&TransportBatched<float>);
+    if (precision == kFP64) {
+        return diagnostics ? reinterpret_cast<const void*>(&TransportBatched<double, true>)
+                           : reinterpret_cast<const void*>(&TransportBatched<double, false>);
+    }
+    return diagnostics ? reinterpret_cast<const void*>(&TransportBatched<float, true>)
+                       : reinterpret_cast<const void*>(&TransportBatched<float, false>);
 }
 
 const void* ZeroCountersKernel() { return reinterpret_cast<const void*>(&ZeroCounters); }
 
 cudaError_t ConfigureTransportKernels(std::size_t sharedBytes) {
     for (int precision = 0; precision < 2; ++precision) {
-        for (int form = 0; form < 2; ++form) {
+        for (int form = 0; form < 4; ++form) {  // kBatched, kPlain, each with and without kWithDiagnostics
             const cudaError_t error{cudaFuncSetAttribute(TransportKernel(precision, form),
                                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                          static_cast<int>(sharedBytes))};

@@ -198,7 +198,8 @@ typedef struct g4b_config {
     float boundary_tolerance_mm;     /* 0 -> 1e-4 (PhotonTransportConfig.hpp:31) */
     uint32_t precision;              /* g4b_precision */
     uint32_t launch_form;            /* g4b_launch_form */
-    uint32_t enable_performance_diagnostics;
+    uint32_t enable_performance_diagnostics; /* 1: count coincident-face retraces and hits
+                                                (g4b_performance), as the reference does only then */
     uint32_t ordered_detections;     /* 1: detections in flattened photon order, as the reference returns them */
     uint64_t hit_capacity;           /* device hit-buffer rows; 0 -> photons of the batch */
     uint32_t block_size;             /* 0 -> autotuned/default (256) */

@@ -59,7 +59,7 @@ def test_engine_matches_oracle_bit_for_bit(oracle, case, precision, form):
     scene = scenes.crystal_sipm_scene()
     batch = scenes.workload(name, event_count=events, seed=7)
     config = dict(seed=20250101, precision=precision, launch_form=form)
-    engine = run_engine(scene, batch, **config)
+    engine = run_engine(scene, batch, enable_performance_diagnostics=True, **config)
     reference = oracle.transport(scene, batch, PhotonTransportConfig(**config))
     assert engine.statistics["captured_count"] == batch.photon_count
     assert_detections_equal(engine.detections, reference.detections)
@@ -67,6 +67,12 @@ def test_engine_matches_oracle_bit_for_bit(oracle, case, precision, form):
     assert engine.performance["total_bounce_count"] == reference.total_bounce_count
     assert engine.performance["coincident_candidate_trace_count"] == reference.coincident[0]
     assert engine.performance["coincident_candidate_hit_count"] == reference.coincident[1]
+    # without diagnostics the kernel leaves the coincidence counters out and
+    # transports identically
+    quiet = run_engine(scene, batch, **config)
+    assert quiet.detections.tobytes() == engine.detections.tobytes()
+    assert quiet.performance["total_bounce_count"] == engine.performance["total_bounce_count"]
+    assert quiet.performance["coincident_candidate_trace_count"] == 0
 
 
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
