@@ -231,7 +231,7 @@ std::size_t SharedBytes(const g4b_handle& h, int form, std::uint32_t blockSize) 
         const bool fp64{h.config.precision == G4B_PRECISION_FP64};
         const std::size_t queue{fp64 ? g4b::kQueueBytesFP64 : g4b::kQueueBytesFP32};
         const std::size_t ring{fp64 ? g4b::kRingBytesFP64 : g4b::kRingBytesFP32};
-        bytes += (queue + ring) * (blockSize / 32U);
+        bytes += (queue + ring) * (blockSize / 32U) + g4b::kLaneTallyBytes * blockSize;
     }
     return bytes;
 }
@@ -545,7 +545,8 @@ void BuildScene(g4b_handle& h, const g4b_scene& scene) {
     h.dScene.Ensure(blob.size(), "cudaMalloc scene");
     Check(cudaMemcpy(h.dScene.pointer, blob.data(), blob.size(), cudaMemcpyHostToDevice), "cudaMemcpy scene");
     Check(g4b::ConfigureTransportKernels(((blob.size() + 15U) & ~std::size_t{15}) +
-                                         8U * (g4b::kQueueBytesFP64 + g4b::kRingBytesFP64)),
+                                         8U * (g4b::kQueueBytesFP64 + g4b::kRingBytesFP64) +
+                                         256U * g4b::kLaneTallyBytes),
           "cudaFuncSetAttribute shared memory");
     h.sceneBlob = std::move(blob);
     h.sceneBytes = static_cast<std::uint32_t>(h.sceneBlob.size());

@@ -105,6 +105,9 @@ constexpr std::uint32_t kQueueBytesFP64 = 10U * 32U * 8U + 32U * 8U + 5U * 32U *
 constexpr std::uint32_t kFresnelRingEntries = 48;
 constexpr std::uint32_t kRingBytesFP32 = kFresnelRingEntries * (12U * 4U + 8U + 7U * 4U);  // 4032
 constexpr std::uint32_t kRingBytesFP64 = kFresnelRingEntries * (12U * 8U + 8U + 7U * 4U);  // 6336
+// Per-thread event counters and bounce total of the batched form, kept in
+// shared memory instead of registers (they change once per photon).
+constexpr std::uint32_t kLaneTallyBytes = 40;
 
 // Per-event counters (DeviceEventTransportStats, OptiXDeviceData.cuh:159-167),
 // padded to 64 bytes.

@@ -83,6 +83,15 @@ struct LaneCounters {
     }
 };
 
+// A thread's event counters and bounce total in the batched form, in shared
+// memory: they change once per photon, and keeping them out of registers
+// leaves more of the register budget to the step loop.
+struct LaneTally {
+    LaneCounters counters;
+    unsigned long long bounces;
+};
+static_assert(sizeof(LaneTally) == kLaneTallyBytes, "tally layout");
+
 // Largest emission e in [begin, end) with offsets[e] <= slot (FindEmissionIndex, :304-320).
 __device__ __forceinline__ std::uint32_t FindEmission(const std::uint32_t* __restrict__ offsets, std::uint32_t begin,
                                                       std::uint32_t end, std::uint32_t slot) {
@@ -363,8 +372,12 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
     const std::uint32_t sceneEnd{(p.sceneBytes + 15U) & ~15U};
     WarpQueue<R>& queue{
         *reinterpret_cast<WarpQueue<R>*>(gShared + sceneEnd + (threadIdx.x >> 5U) * sizeof(WarpQueue<R>))};
-    FresnelRing<R>& ring{*reinterpret_cast<FresnelRing<R>*>(gShared + sceneEnd + (blockDim.x >> 5U) * sizeof(WarpQueue<R>) +
+    const std::uint32_t warps{blockDim.x >> 5U};
+    FresnelRing<R>& ring{*reinterpret_cast<FresnelRing<R>*>(gShared + sceneEnd + warps * sizeof(WarpQueue<R>) +
                                                             (threadIdx.x >> 5U) * sizeof(FresnelRing<R>))};
+    LaneTally& tally{*reinterpret_cast<LaneTally*>(gShared + sceneEnd +
+                                                   warps * (sizeof(WarpQueue<R>) + sizeof(FresnelRing<R>)) +
+                                                   threadIdx.x * sizeof(LaneTally))};
     constexpr std::uint32_t kRing{FresnelRing<R>::kEntries};
     std::uint32_t readyHead{0U};
     std::uint32_t pendingHead{0U};
@@ -378,10 +391,10 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
     bool workDone{false};
     bool alive{false};
     Photon<R> photon{};
-    LaneCounters counters{};
+    LaneCounters& counters{tally.counters};
     counters.eventIndex = kInvalidID;
     counters.Reset();
-    unsigned long long laneBounces{0ULL};
+    tally.bounces = 0ULL;
     std::uint32_t coincidentTraces{0U};
     std::uint32_t coincidentHits{0U};
 
@@ -400,7 +413,7 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
                     alive = true;
                 } else {  // truncated by the Fresnel step's bounce
                     counters.Finish(status, photon.bounce);
-                    laneBounces += photon.bounce;
+                    tally.bounces += photon.bounce;
                     RecordFate(p, photon.slot, status, photon.bounce, photon.time);
                 }
             }
@@ -515,7 +528,9 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
         }
         WriteHits(alive && result == kDetected, photon, extras.sensorID, p, lane);
         if (alive) {
-            counters.zeroStep += extras.zeroSteps;
+            if (extras.zeroSteps != 0U) {
+                counters.zeroStep += extras.zeroSteps;
+            }
             if constexpr (kDiagnostics) {
                 coincidentTraces += extras.coincidentTraces;
                 coincidentHits += extras.coincidentHits;
@@ -525,7 +540,7 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
             } else if (result != kContinue) {
                 const std::uint32_t bounces{result == kTruncated ? photon.bounce : photon.bounce + 1U};
                 counters.Finish(result, bounces);
-                laneBounces += bounces;
+                tally.bounces += bounces;
                 RecordFate(p, photon.slot, result, bounces, photon.time);
                 alive = false;
             }
@@ -536,7 +551,7 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
         }
     }
     counters.Flush(p.events);
-    FlushRunCounters(p, laneBounces, coincidentTraces, coincidentHits, lane);
+    FlushRunCounters(p, tally.bounces, coincidentTraces, coincidentHits, lane);
 }
 
 template<class R, bool kDiagnostics>
