@@ -132,6 +132,16 @@ __device__ __forceinline__ Dual<double> Uniform<Dual<double>>(unsigned long long
     return Dual<double>(Uniform<double>(seed, key, bounce, process, draw));
 }
 
+// UniformFromWord for plain and dual numbers (a draw carries no derivative).
+template<class R>
+__device__ __forceinline__ R UniformSample(std::uint32_t word) {
+    if constexpr (IsDualType<R>::value) {
+        return R(UniformFromWord<decltype(R{}.v)>(word));
+    } else {
+        return UniformFromWord<R>(word);
+    }
+}
+
 // The value of a plain or dual number, and the value of one with the
 // derivative of another (used where the value comes from an FP64 side
 // computation the dual arithmetic cannot see).
