@@ -99,12 +99,13 @@ static_assert(sizeof(PackedScene) % 16 == 0, "scene blob must stay 16-byte align
 constexpr std::uint32_t kQueueBytesFP32 = 10U * 32U * 4U + 32U * 8U + 5U * 32U * 4U;  // 2176
 constexpr std::uint32_t kQueueBytesFP64 = 10U * 32U * 8U + 32U * 8U + 5U * 32U * 4U;  // 3456
 // Per-warp ring of photons stopped at a Fresnel boundary (pending) or done
-// with it (ready): 12 real columns, FP64 time, 7 u32 columns, 48 entries (a
-// batch of 32 plus room to keep parking while ready photons drain; 64 left
-// 128-thread blocks one block per SM short of 24 warps).
-constexpr std::uint32_t kFresnelRingEntries = 48;
-constexpr std::uint32_t kRingBytesFP32 = kFresnelRingEntries * (12U * 4U + 8U + 7U * 4U);  // 4032
-constexpr std::uint32_t kRingBytesFP64 = kFresnelRingEntries * (12U * 8U + 8U + 7U * 4U);  // 6336
+// with it (ready): 12 real columns, FP64 time, 7 u32 columns, 40 entries (a
+// batch of 32 plus room to keep parking while ready photons drain; with 40,
+// three 256-thread blocks use at most 196 KB of shared memory per SM, which
+// leaves the L1 data cache 60 KB instead of 28 KB).
+constexpr std::uint32_t kFresnelRingEntries = 40;
+constexpr std::uint32_t kRingBytesFP32 = kFresnelRingEntries * (12U * 4U + 8U + 7U * 4U);  // 3360
+constexpr std::uint32_t kRingBytesFP64 = kFresnelRingEntries * (12U * 8U + 8U + 7U * 4U);  // 5280
 // Per-thread event counters and bounce total of the batched form, kept in
 // shared memory instead of registers (they change once per photon).
 constexpr std::uint32_t kLaneTallyBytes = 40;
