@@ -502,6 +502,10 @@ void BuildScene(g4b_handle& h, const g4b_scene& scene) {
                         const double planeFirst{sideFirst == 0 ? first.lo[axis] : first.hi[axis]};
                         const double planeSecond{sideSecond == 0 ? second.lo[axis] : second.hi[axis]};
                         if (std::fabs(planeFirst - planeSecond) <= tolerance) {
+                            // One plane for both faces. Centre +- half in float can leave
+                            // touching faces an ulp apart, and along a grazing ray an ulp
+                            // in z is far more than the coincidence window in distance.
+                            (sideSecond == 0 ? second.lo[axis] : second.hi[axis]) = static_cast<float>(planeFirst);
                             packed->volumes[i].coincidentFaces |= static_cast<std::uint8_t>(1U << (2 * axis + sideFirst));
                             packed->volumes[j].coincidentFaces |= static_cast<std::uint8_t>(1U << (2 * axis + sideSecond));
                             packed->volumes[i].mayCoincide = 1;
