@@ -17,16 +17,14 @@ resolves nothing there: they use steps of 1e-2 and must lie within four
 standard errors. The decay-time derivative of the mean time is large and is
 held to 2 %.
 
-The refractive-index derivative has two known limits:
-  - geometric discontinuities are not estimated: in the standard detector a
-    refracted ray moving across the edge of the 3x3 mm grease changes its
-    fate, and that boundary term is about half of dN/dn there, so dN/dn is
-    checked on a coupling layer wider than the crystal;
-  - with many Fresnel encounters per photon (a reflective wrapper) the replay
-    measures 5-8 % below the finite difference, a deficit that does not shrink
-    with statistics or with the step (finite differences from 1e-4 to 3e-3
-    agree to 0.5 %); with a single encounter per photon (a black wrapper) the
-    two agree to 2 %.
+The refractive-index derivative omits geometric boundary terms: when a
+change of n moves a refracted ray across the edge of a face, the photon's
+fate changes discontinuously, and neither a pathwise nor a score term sees
+that. Near the critical angle the rays refracted into the 0.1 mm grease run
+almost parallel to it and travel far sideways, so the edges of the coupling
+layer matter: with the standard 3x3 mm layer the edge term is about half of
+dN/dn, with a 40 mm layer about 3 %. dN/dn is therefore checked on a 1 m
+coupling layer, where grazing rays reach the SiPM before any edge.
 """
 import numpy as np
 import pytest
@@ -55,7 +53,8 @@ def evaluate(theta, base, coupling_half_mm=None, gradients=False):
     n, length, reflectivity, tau = (float(x) for x in theta)
     scene = scenes.crystal_sipm_scene(scenes.DetectorParameters(
         crystal_rindex=n, crystal_abs_length_mm=length, wrapper_reflectivity=reflectivity,
-        coupling_half_xy_mm=coupling_half_mm))
+        coupling_half_xy_mm=coupling_half_mm,
+        world_half_mm=50.0 if coupling_half_mm is None else max(50.0, 2.0 * coupling_half_mm)))
     batch = with_decay(base, tau)
     with TransportHost(PhotonTransportConfig(seed=SEED, precision="fp32")) as host:
         host.enqueue_emissions(scene, batch)
@@ -142,26 +141,25 @@ def test_absorption_reflectivity_and_decay_gradients(base_batch, theta0):
 
 
 def test_index_gradient_with_one_fresnel_choice_per_photon():
-    """Black wrapper, wide coupling layer: every detected photon made exactly one
+    """Black wrapper, 1 m coupling layer: every detected photon made exactly one
     Fresnel choice, so dN/dn is the expectation of 0.3 dT/dn and must match."""
     base = scenes.workload("gradients", event_count=20000, seed=7, cerenkov=False)
     theta0 = (1.82, 400.0, 0.0, 40.0)
-    grad_detected, grad_time = gradients_of(theta0, base, coupling_half_mm=40.0)
-    dn, dn_se, _, _ = central_differences(theta0, base, 40.0, 0)
-    _, _, dt, dt_se = central_differences(theta0, base, 40.0, 0, TIME_STEP)
+    grad_detected, grad_time = gradients_of(theta0, base, coupling_half_mm=1000.0)
+    dn, dn_se, _, _ = central_differences(theta0, base, 1000.0, 0)
+    _, _, dt, dt_se = central_differences(theta0, base, 1000.0, 0, TIME_STEP)
     print(f"\ndN/dn replay {grad_detected[0]:.6g} FD {dn:.6g} +- {dn_se:.3g};"
           f" d<t>/dn replay {grad_time[0]:.5g} FD {dt:.5g} +- {dt_se:.3g}")
     assert agrees(grad_detected[0], dn, dn_se), (grad_detected[0], dn, dn_se)
     assert agrees(grad_time[0], dt, dt_se, sigmas=4.0), (grad_time[0], dt, dt_se)
 
 
-def test_index_gradient_with_a_reflective_wrapper_stays_within_its_known_deficit(base_batch):
-    """Reflective wrapper, wide coupling layer: the measured deficit of the
-    replay (5-8 % below the finite difference) must not grow."""
+def test_index_gradient_with_a_reflective_wrapper(base_batch):
+    """Reflective wrapper, 1 m coupling layer: photons meet the crystal-grease
+    face many times, and the replay's alternate branches and pathwise
+    polarisation derivatives must add up to the finite difference."""
     theta0 = (1.82, 400.0, 0.95, 40.0)
-    grad_detected, _ = gradients_of(theta0, base_batch, coupling_half_mm=40.0)
-    dn, dn_se, _, _ = central_differences(theta0, base_batch, 40.0, 0)
-    ratio = grad_detected[0] / dn
-    print(f"\ndN/dn replay {grad_detected[0]:.6g} FD {dn:.6g} +- {dn_se:.3g} ratio {ratio:.4f}")
-    assert dn < 0.0 and grad_detected[0] < 0.0
-    assert 0.88 <= ratio <= 1.0 + 3.0 * dn_se / abs(dn), ratio
+    grad_detected, _ = gradients_of(theta0, base_batch, coupling_half_mm=1000.0)
+    dn, dn_se, _, _ = central_differences(theta0, base_batch, 1000.0, 0)
+    print(f"\ndN/dn replay {grad_detected[0]:.6g} FD {dn:.6g} +- {dn_se:.3g} ratio {grad_detected[0] / dn:.4f}")
+    assert agrees(grad_detected[0], dn, dn_se), (grad_detected[0], dn, dn_se)
