@@ -138,11 +138,9 @@ struct RunCounters {
 // 0 refractive index, 1 absorption length, 2 reflectivity, 3 decay time.
 struct GradientSums {
     double detected;       // N
-    double time;           // sum of arrival times
-    double score[4];       // sum of S_j (score + pathwise log-probability terms)
-    double timeScore[4];   // sum of t S_j + dt/dtheta_j
-    unsigned long long mismatches;  // unused (the host compares detected counts)
-    unsigned long long reserved;
+    double time;           // sum of arrival times of the detected photons
+    double score[4];       // dN/dtheta_j: score, pathwise and alternate-branch terms
+    double timeScore[4];   // d(sum of arrival times)/dtheta_j
 };
 
 // Compacted hits, structure of arrays, `capacity` rows each.
