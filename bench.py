@@ -51,7 +51,57 @@ def parse_args():
     parser.add_argument("--no-plain", action="store_true")
     parser.add_argument("--no-e2e", action="store_true")
     parser.add_argument("--no-autotune", action="store_true")
+    parser.add_argument("--no-scheduler", action="store_true")
+    parser.add_argument("--scheduler-events", type=int, default=5000,
+                        help="events of the same workload streamed through the batch scheduler")
     return parser.parse_args()
+
+
+def scheduler_leg(scene, events: int, local: int, producers: int = 8, window: int = 64) -> dict:
+    """Events streamed one at a time through the batch scheduler
+    (include/g4b_scheduler.h) by `producers` native threads
+    (g4b_scheduler_replay), each keeping at most `window` results
+    outstanding (the reference's maxPendingEvents per worker,
+    PhotonTransportConfig.hpp:36): pipelined (two batches in flight) and in the reference's
+    serial order at the reference's batch target, and pipelined at a larger
+    target. Host wall clock from the first submission to the last result,
+    after one warm-up pass."""
+    from g4go_b200 import PhotonTransportConfig, scenes
+    from g4go_b200.scheduler import BatchSchedulerConfig, OpticalBatchScheduler, OpticalSubmission
+
+    batch = scenes.workload("batched", event_count=events, seed=5)
+    indices = batch.emission_event_indices
+    if np.any(np.diff(indices.astype(np.int64)) < 0):
+        order = np.argsort(indices, kind="stable")
+        emissions, indices = batch.emissions[order], indices[order]
+    else:
+        emissions = batch.emissions
+    bounds = np.searchsorted(indices, np.arange(len(batch.event_ids) + 1))
+    submissions = [OpticalSubmission(int(event_id), emissions[bounds[i]:bounds[i + 1]])
+                   for i, event_id in enumerate(batch.event_ids)]
+    photons = int(sum(sub.photon_count for sub in submissions))
+    out = {"unit": UNIT, "events": len(submissions), "photons": photons, "producers": producers,
+           "window": window, "timing": "host wall clock, first submission to last result, after a warm-up pass"}
+    runs = (("pipelined", BatchSchedulerConfig(enable_performance_diagnostics=True)),
+            ("serial", BatchSchedulerConfig(serial=True, enable_performance_diagnostics=True)),
+            ("pipelined_4M", BatchSchedulerConfig(target_photons_per_batch=4_000_000, max_queued_photons=8_000_000,
+                                                  enable_performance_diagnostics=True)))
+    for name, batching in runs:
+        config = PhotonTransportConfig(seed=7, device=local)
+        with OpticalBatchScheduler(config, scene, batching) as scheduler:
+            scheduler.replay(submissions, producers, window)  # warm-up: engine handles, graphs, staging
+            before = scheduler.batch_statistics()
+            detections, seconds = scheduler.replay(submissions, producers, window)
+            after = scheduler.batch_statistics()
+        out[name] = {"value": photons / seconds, "seconds": seconds, "detections": detections,
+                     "target_photons_per_batch": batching.target_photons_per_batch,
+                     "batches": after["batch_count"] - before["batch_count"],
+                     "overlapped_batches": after["overlapped_batch_count"] - before["overlapped_batch_count"],
+                     "kernel_ms": after["performance"]["kernel_ms"] - before["performance"]["kernel_ms"],
+                     "transport_thread_ms": {key: after[f"scheduler_{key}_ms"] - before[f"scheduler_{key}_ms"]
+                                             for key in ("input_wait", "gpu_wait", "batch_flatten")}}
+    out["value"] = out["pipelined"]["value"]
+    return out
 
 
 def distributed():
@@ -329,6 +379,10 @@ def bench_ours(args, world, rank, local):
     clocks = sampler.summary()
     host.close()
 
+    streamed = None
+    if not args.no_scheduler and rank == 0 and world == 1:
+        streamed = scheduler_leg(scene, min(args.scheduler_events, args.events), local)
+
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         cpu_photons, cpu_seconds, cores = run_oracle_sample(batch, scene, args.cpu_seconds, seed=7)
@@ -389,6 +443,7 @@ def bench_ours(args, world, rank, local):
         "plain_fp64": plain,
         "batched_over_plain": (value / world / plain["value"]) if plain else None,
         "cpu_baseline": cpu,
+        "scheduler": streamed,
     }
     print(json.dumps(line), flush=True)
     if world > 1:

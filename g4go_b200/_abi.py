@@ -1,4 +1,4 @@
-"""ctypes view of the engine's C ABI (include/g4b.h, include/g4b_synth.h).
+"""ctypes view of the engine's C ABI (include/g4b.h, include/g4b_scheduler.h, include/g4b_synth.h).
 
 Loads g4go_b200/_lib/libg4b.so, the sm_100a build of the engine. There is no
 fallback: if the library is missing it is built with nvcc, and if that is
@@ -254,6 +254,60 @@ class Output(C.Structure):
     ]
 
 
+class SchedulerConfig(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_uint32),
+        ("target_photons_per_batch", C.c_uint32),
+        ("max_events_per_batch", C.c_uint32),
+        ("max_queued_photons", C.c_uint32),
+        ("max_queued_submissions", C.c_uint32),
+        ("batch_collection_timeout_ms", C.c_uint32),
+        ("enable_performance_diagnostics", C.c_uint32),
+        ("serial", C.c_uint32),
+        ("reserved", C.c_uint32 * 8),
+    ]
+
+
+class BatchStatistics(C.Structure):
+    _fields_ = [
+        ("batch_count", C.c_uint64),
+        ("event_count", C.c_uint64),
+        ("photon_count", C.c_uint64),
+        ("max_batch_photon_count", C.c_uint64),
+        ("max_batch_event_count", C.c_uint64),
+        ("queue_high_water_mark", C.c_uint64),
+        ("min_batch_photon_count", C.c_uint64),
+        ("total_queue_wait_count", C.c_uint64),
+        ("scheduler_input_wait_ms", C.c_double),
+        ("scheduler_gpu_wait_ms", C.c_double),
+        ("scheduler_queue_wait_ms", C.c_double),
+        ("scheduler_batch_flatten_ms", C.c_double),
+        ("scheduler_batch_flatten_bytes", C.c_uint64),
+        ("overlapped_batch_count", C.c_uint64),
+        ("performance", Performance),
+    ]
+
+
+# g4b_transport_ops: a transport the scheduler drives (include/g4b_scheduler.h).
+TRANSPORT_ENQUEUE = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32,
+                                C.POINTER(C.c_uint32))
+TRANSPORT_POLL = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_int))
+TRANSPORT_QUERY = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32))
+TRANSPORT_COMPLETE = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(Output))
+TRANSPORT_LAST_ERROR = C.CFUNCTYPE(C.c_void_p, C.c_void_p)
+
+
+class TransportOps(C.Structure):
+    _fields_ = [
+        ("context", C.c_void_p),
+        ("enqueue", TRANSPORT_ENQUEUE),
+        ("poll", TRANSPORT_POLL),
+        ("query", TRANSPORT_QUERY),
+        ("complete", TRANSPORT_COMPLETE),
+        ("last_error", TRANSPORT_LAST_ERROR),
+    ]
+
+
 class TuneResult(C.Structure):
     _fields_ = [
         ("block_size", C.c_uint32),
@@ -332,6 +386,7 @@ SIGNATURES = {
     "g4b_enqueue": (_I32, [_VP, _VP, _U32, _PU32, _U32, _PU32]),
     "g4b_relaunch": (_I32, [_VP]),
     "g4b_query_oldest": (_I32, [_VP, _PU64, _PU32]),
+    "g4b_poll_oldest": (_I32, [_VP, C.POINTER(C.c_int)]),
     "g4b_complete": (_I32, [_VP, C.POINTER(Output)]),
     "g4b_get_stream": (_I32, [_VP, C.POINTER(_VP)]),
     "g4b_photon_fates": (_I32, [_VP, _PU32, _PD, _U64, _PU64]),
@@ -345,6 +400,18 @@ SIGNATURES = {
     "g4b_host_free": (_I32, [_VP]),
     "g4b_order_detections_static": (_I32, [_VP, _VP, _U64, _U32, _VP, _VP]),
     "g4b_abi_version": (_U32, []),
+    "g4b_scheduler_create": (_I32, [C.POINTER(Config), C.POINTER(Scene), C.POINTER(SchedulerConfig), C.POINTER(_VP)]),
+    "g4b_scheduler_create_with_transport": (
+        _I32,
+        [C.POINTER(TransportOps), _U32, C.POINTER(SchedulerConfig), C.POINTER(_VP)],
+    ),
+    "g4b_scheduler_submit": (_I32, [_VP, _U32, _VP, _U32, _U64, C.POINTER(Statistics), _PU64]),
+    "g4b_scheduler_wait": (_I32, [_VP, _U64, C.c_int64, C.POINTER(Output)]),
+    "g4b_scheduler_end_run": (_I32, [_VP]),
+    "g4b_scheduler_statistics": (_I32, [_VP, C.POINTER(Statistics), C.POINTER(BatchStatistics)]),
+    "g4b_scheduler_destroy": (_I32, [_VP]),
+    "g4b_scheduler_replay": (_I32, [_VP, _VP, _PU64, _PU32, _U32, _U32, _U32, _PU64, _PD]),
+    "g4b_scheduler_last_error": (C.c_char_p, []),
     "g4b_synth_electrons": (_I32, [C.POINTER(SynthParams), C.POINTER(_VP)]),
     "g4b_synth_isotropic_photons": (
         _I32,

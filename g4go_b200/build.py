@@ -21,6 +21,7 @@ SOURCES = [
     PACKAGE / "csrc" / "transport_kernels.cu",
     PACKAGE / "csrc" / "engine.cpp",
     PACKAGE / "csrc" / "synth.cpp",
+    PACKAGE / "csrc" / "scheduler.cpp",
 ]
 HEADERS = [
     PACKAGE / "csrc" / "g4b_device.cuh",
@@ -28,6 +29,7 @@ HEADERS = [
     PACKAGE / "csrc" / "kernels.h",
     PACKAGE.parent / "include" / "g4b.h",
     PACKAGE.parent / "include" / "g4b_synth.h",
+    PACKAGE.parent / "include" / "g4b_scheduler.h",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

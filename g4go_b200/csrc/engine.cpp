@@ -1275,6 +1275,32 @@ int g4b_query_oldest(g4b_handle* h, uint64_t* detectionCount, uint32_t* eventCou
     });
 }
 
+int g4b_poll_oldest(g4b_handle* h, int* ready) {
+    if (h == nullptr || ready == nullptr) {
+        gHandlelessError = "null argument";
+        return G4B_ERR_INVALID_ARGUMENT;
+    }
+    return Guard(h, [&]() {
+        if (!h->busy) {
+            Throw(G4B_ERR_LOGIC, "transport queue is empty");
+        }
+        if (h->metadataReady || h->photonCount == 0) {
+            *ready = 1;
+            return;
+        }
+        Check(cudaSetDevice(h->device), "cudaSetDevice");
+        const cudaError_t status{cudaEventQuery(h->metadataReadyEvent)};
+        if (status == cudaErrorNotReady) {
+            // not an error: leave no trace of it for later launch checks
+            static_cast<void>(cudaGetLastError());
+            *ready = 0;
+            return;
+        }
+        Check(status, "cudaEventQuery metadata");
+        *ready = 1;
+    });
+}
+
 int g4b_complete(g4b_handle* h, g4b_output* output) {
     if (h == nullptr) {
         gHandlelessError = "null handle";

@@ -340,6 +340,13 @@ int g4b_relaunch(g4b_handle* handle);
  * reports how many detections and events g4b_complete will return. */
 int g4b_query_oldest(g4b_handle* handle, uint64_t* detection_count, uint32_t* event_count);
 
+/* Without waiting: *ready = 1 once the pending batch's transport and metadata
+ * copy have finished on the device (g4b_query_oldest and g4b_complete will then
+ * not block on the GPU), else 0. No counterpart in the reference, whose
+ * CompleteOldestBatch only blocks; the batch scheduler (g4b_scheduler.h) polls
+ * it to keep collecting submissions while a batch runs. */
+int g4b_poll_oldest(g4b_handle* handle, int* ready);
+
 /* OptiXTransportHost::CompleteOldestBatch (OptiXTransportHost.cpp:779-883):
  * waits for the pending batch, copies the compacted hits back and fills
  * *output. If output->detection_capacity or event_capacity is too small it
