@@ -38,7 +38,7 @@ def test_record_layouts_match_the_reference(tmp_path):
 
     program = tmp_path / "layout.c"
     program.write_text(
-        '#include <stddef.h>\n#include <stdio.h>\n#include "g4b.h"\n#include "g4b_synth.h"\n'
+        '#include <stddef.h>\n#include <stdio.h>\n#include "g4b.h"\n#include "g4b_synth.h"\n#include "g4b_scheduler.h"\n'
         "int main(void){\n"
         ' printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n",'
         " sizeof(g4b_optical_emission), sizeof(g4b_photon_detection), sizeof(g4b_config), sizeof(g4b_property),"
@@ -48,11 +48,13 @@ def test_record_layouts_match_the_reference(tmp_path):
         ' printf("%zu %zu %zu %zu\\n", offsetof(g4b_optical_emission, event_id),'
         " offsetof(g4b_optical_emission, photon_count), offsetof(g4b_photon_detection, sensor_id),"
         " offsetof(g4b_config, hit_capacity));\n"
+        ' printf("%zu %zu %zu %zu\\n", sizeof(g4b_scheduler_config), sizeof(g4b_batch_statistics),'
+        " sizeof(g4b_transport_ops), offsetof(g4b_batch_statistics, performance));\n"
         " return 0; }\n"
     )
     exe = tmp_path / "layout"
     subprocess.run(["gcc", "-std=c11", "-I", str(ROOT / "include"), str(program), "-o", str(exe)], check=True)
-    first, second = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines()
+    first, second, third = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines()
     sizes = list(map(int, first.split()))
     offsets = list(map(int, second.split()))
     assert sizes[0] == 128 and sizes[1] == 48  # PhotonTransport.hpp:177-178
@@ -67,6 +69,9 @@ def test_record_layouts_match_the_reference(tmp_path):
     assert offsets[1] == 96 == _abi.EMISSION_DTYPE.fields["photon_count"][1]
     assert offsets[2] == 40 == _abi.DETECTION_DTYPE.fields["sensor_id"][1]
     assert offsets[3] == _abi.Config.hit_capacity.offset
+    # the batch scheduler's records (include/g4b_scheduler.h)
+    assert list(map(int, third.split())) == [C.sizeof(_abi.SchedulerConfig), C.sizeof(_abi.BatchStatistics),
+                                             C.sizeof(_abi.TransportOps), _abi.BatchStatistics.performance.offset]
 
 
 def test_cpp_shim_compiles(tmp_path):
