@@ -63,8 +63,7 @@ def scheduler_leg(scene, events: int, local: int, producers: int = 8, window: in
     (g4b_scheduler_replay), each keeping at most `window` results
     outstanding (the reference's maxPendingEvents per worker,
     PhotonTransportConfig.hpp:36): pipelined (two batches in flight) and in the reference's
-    serial order at the reference's batch target, and pipelined at a larger
-    target. Host wall clock from the first submission to the last result,
+    serial order, both at the reference's batch target. Host wall clock from the first submission to the last result,
     after one warm-up pass."""
     from g4go_b200 import PhotonTransportConfig, scenes
     from g4go_b200.scheduler import BatchSchedulerConfig, OpticalBatchScheduler, OpticalSubmission
@@ -83,9 +82,7 @@ def scheduler_leg(scene, events: int, local: int, producers: int = 8, window: in
     out = {"unit": UNIT, "events": len(submissions), "photons": photons, "producers": producers,
            "window": window, "timing": "host wall clock, first submission to last result, after a warm-up pass"}
     runs = (("pipelined", BatchSchedulerConfig(enable_performance_diagnostics=True)),
-            ("serial", BatchSchedulerConfig(serial=True, enable_performance_diagnostics=True)),
-            ("pipelined_4M", BatchSchedulerConfig(target_photons_per_batch=4_000_000, max_queued_photons=8_000_000,
-                                                  enable_performance_diagnostics=True)))
+            ("serial", BatchSchedulerConfig(serial=True, enable_performance_diagnostics=True)))
     for name, batching in runs:
         config = PhotonTransportConfig(seed=7, device=local)
         with OpticalBatchScheduler(config, scene, batching) as scheduler:

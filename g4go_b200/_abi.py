@@ -264,7 +264,8 @@ class SchedulerConfig(C.Structure):
         ("batch_collection_timeout_ms", C.c_uint32),
         ("enable_performance_diagnostics", C.c_uint32),
         ("serial", C.c_uint32),
-        ("reserved", C.c_uint32 * 8),
+        ("batches_in_flight", C.c_uint32),
+        ("reserved", C.c_uint32 * 7),
     ]
 
 

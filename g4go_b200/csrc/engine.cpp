@@ -193,6 +193,7 @@ struct g4b_handle {
     std::uint32_t blockSize{256};
     std::uint32_t blocksPerSM{0};
     std::uint32_t chunk{512};
+    bool chunkAdaptive{false};  // chunk_photons left at 0 and no autotune: shrink the chunk for small batches
 
     // Graph for the batched form: [ZeroCounters] -> [TransportBatched].
     cudaGraph_t graph{nullptr};
@@ -694,10 +695,18 @@ std::uint64_t DefaultHitRows(std::uint64_t photons) {
 // Runs the staged batch once: counters zeroed, transport, metadata back.
 void RunStaged(g4b_handle& h) {
     EnsureHitCapacity(h, h.config.hit_capacity != 0 ? h.config.hit_capacity : DefaultHitRows(h.photonCount));
-    const LaunchParams base{BaseParams(h)};
+    LaunchParams base{BaseParams(h)};
     Check(cudaEventRecord(h.kernelTimer.start, h.stream), "cudaEventRecord");
     if (Form(h) == g4b::kBatched) {
         const unsigned grid{BatchedGrid(h)};
+        if (h.chunkAdaptive) {
+            // at least eight queue grabs per warp, so that a small batch's
+            // photons (and its tail) are shared out over every warp; never
+            // more than the configured chunk
+            const std::uint64_t warps{static_cast<std::uint64_t>(grid) * (h.blockSize / 32U)};
+            const std::uint64_t perWarp{h.photonCount / (warps * 8U)};
+            base.chunk = RoundChunk(static_cast<std::uint32_t>(std::clamp<std::uint64_t>(perWarp, 32U, h.chunk)));
+        }
         if (h.config.use_cuda_graph != 0) {
             LaunchBatchedGraph(h, base, grid);
         } else {
@@ -1167,6 +1176,7 @@ int g4b_create(const g4b_config* config, g4b_handle** outHandle) {
         handle->blockSize = config->block_size != 0 ? config->block_size : 256;
         handle->blocksPerSM = config->blocks_per_sm;
         handle->chunk = RoundChunk(config->chunk_photons != 0 ? config->chunk_photons : 512);
+        handle->chunkAdaptive = config->chunk_photons == 0;
         *outHandle = handle.release();
     });
 }
@@ -1432,6 +1442,7 @@ int g4b_autotune(g4b_handle* h, const uint32_t* blockSizes, uint32_t nBlockSizes
         h->blockSize = best.block_size;
         h->blocksPerSM = best.blocks_per_sm;
         h->chunk = best.chunk_photons;
+        h->chunkAdaptive = false;
         if (result != nullptr) {
             *result = best;
         }

@@ -219,6 +219,8 @@ void ApplyDefaults(g4b_scheduler_config& c) {
     if (c.max_queued_photons == 0U) c.max_queued_photons = 2000000U;
     if (c.max_queued_submissions == 0U) c.max_queued_submissions = 1024U;
     if (c.batch_collection_timeout_ms == 0U) c.batch_collection_timeout_ms = 10U;
+    if (c.batches_in_flight == 0U) c.batches_in_flight = 2U;
+    c.batches_in_flight = std::min(c.batches_in_flight, 4U);
 }
 
 template<class F>
@@ -264,7 +266,7 @@ int Start(g4b_scheduler* s, g4b_scheduler** out) {
 void g4b_scheduler::RunTransportThread() {
     try {
         if (ownsEngine) {
-            const std::size_t count{config.serial != 0U ? 1U : 2U};
+            const std::size_t count{config.serial != 0U ? 1U : config.batches_in_flight};
             for (std::size_t i{}; i < count; ++i) {
                 g4b_handle* handle{nullptr};
                 int status{g4b_create(&engineConfig, &handle)};
@@ -715,8 +717,8 @@ int g4b_scheduler_create_with_transport(const g4b_transport_ops* ops, uint32_t o
         tLastError = "ABI version mismatch";
         return G4B_ERR_INVALID_ARGUMENT;
     }
-    if (opsCount < 1U || opsCount > 2U) {
-        tLastError = "a scheduler takes one or two transports";
+    if (opsCount < 1U || opsCount > 4U) {
+        tLastError = "a scheduler takes one to four transports";
         return G4B_ERR_INVALID_ARGUMENT;
     }
     for (uint32_t i{}; i < opsCount; ++i) {

@@ -41,6 +41,7 @@ class BatchSchedulerConfig:
     batch_collection_timeout_ms: int = 10
     enable_performance_diagnostics: bool = False
     serial: bool = False  # the reference's order: retire a batch before collecting the next
+    batches_in_flight: int = 2  # pipelined: engine handles and batches on the GPU at once (at most 4)
 
     def to_c(self) -> _abi.SchedulerConfig:
         config = _abi.SchedulerConfig()
@@ -52,6 +53,7 @@ class BatchSchedulerConfig:
         config.batch_collection_timeout_ms = int(self.batch_collection_timeout_ms)
         config.enable_performance_diagnostics = int(bool(self.enable_performance_diagnostics))
         config.serial = int(bool(self.serial))
+        config.batches_in_flight = int(self.batches_in_flight)
         return config
 
 
@@ -136,7 +138,7 @@ class OpticalBatchScheduler:
 
     transports: objects with enqueue(emissions, event_ids, emission_event_indices),
     poll() -> bool, query() -> (detections, events) and complete(output) driven
-    instead of engine handles (one or two; see g4b_scheduler_create_with_transport)."""
+    instead of engine handles (one to four; see g4b_scheduler_create_with_transport)."""
 
     def __init__(self, config: PhotonTransportConfig | None = None, scene: Scene | None = None,
                  batching: BatchSchedulerConfig | None = None, transports: Sequence | None = None) -> None:

@@ -205,7 +205,9 @@ typedef struct g4b_config {
     uint32_t block_size;             /* 0 -> autotuned/default (256) */
     uint32_t blocks_per_sm;          /* 0 -> from occupancy */
     uint32_t chunk_photons;          /* photons a warp takes from the work queue at a time (rounded up to
-                                        a multiple of 32); 0 -> 512 */
+                                        a multiple of 32); 0 -> 512, or less (down to 32) for a batch
+                                        too small to give every warp eight chunks, until g4b_autotune
+                                        picks one. Photons per thread per grab = chunk / 32. */
     uint32_t use_cuda_graph;         /* 1 -> batched launches replay a captured graph */
     uint32_t record_photon_fates;    /* 1 -> keep a per-photon fate/bounce/time record (diagnostics) */
     uint32_t reserved[7];

@@ -20,11 +20,11 @@
  * checks of CompleteBatch (:243-446).
  *
  * Unlike the reference, which completes a batch before it collects the next
- * one (:579-593), the scheduler drives two engine handles (two streams, two
- * sets of pinned staging) and keeps two batches in flight: it collects and
- * stages batch k+1 while the GPU transports batch k, so k+1's persistent
- * kernel starts on the SMs that k's drained warps leave, and it splits k's
- * output per event while k+1 runs. Every photon's history depends only on its
+ * one (:579-593), the scheduler drives several engine handles (one stream and
+ * one set of pinned staging each) and keeps that many batches in flight: it
+ * collects and stages batch k+1 while the GPU transports batch k, so k+1's
+ * persistent kernel starts on the SMs that k's drained warps leave, and it
+ * splits k's output per event while the later batches run. Every photon's history depends only on its
  * RNG counters, so the batches' composition changes no detection.
  * serial = 1 restores the reference's order on one handle.
  *
@@ -56,7 +56,8 @@ typedef struct g4b_scheduler_config {
     uint32_t batch_collection_timeout_ms;  /* 0 -> 10 */
     uint32_t enable_performance_diagnostics; /* 1: time queue waits and flattening, as the reference does */
     uint32_t serial;                       /* 1: the reference's order (retire batch k before collecting k+1); 0: pipelined */
-    uint32_t reserved[8];
+    uint32_t batches_in_flight;            /* pipelined: engine handles, and batches on the GPU at once; 0 -> 2, at most 4 */
+    uint32_t reserved[7];
 } g4b_scheduler_config;
 
 /* PhotonBatchStatistics (OpticalBatchScheduler.hpp:20-32) plus the scheduler
@@ -105,9 +106,9 @@ typedef struct g4b_transport_ops {
 int g4b_scheduler_create(const g4b_config* engine_config, const g4b_scene* scene,
                          const g4b_scheduler_config* config, g4b_scheduler** out_scheduler);
 
-/* The same scheduler over caller-supplied transports: ops[0..ops_count) (1 or
- * 2; a second one lets two batches be in flight) are copied, and their
- * contexts must outlive the scheduler. */
+/* The same scheduler over caller-supplied transports: ops[0..ops_count) (1 to
+ * 4; each one more lets one more batch be in flight) are copied, and their
+ * contexts must outlive the scheduler. batches_in_flight is ignored. */
 int g4b_scheduler_create_with_transport(const g4b_transport_ops* ops, uint32_t ops_count,
                                         const g4b_scheduler_config* config, g4b_scheduler** out_scheduler);
 

@@ -248,3 +248,15 @@ def test_detections_out_of_photon_order_are_still_routed_per_event():
         assert sorted(got["photon_id"].tolist()) == sorted(want["photon_id"].tolist())
         assert set(got["event_id"].tolist()) <= {e}
     s.close()
+
+
+def test_four_transports_rotate_in_order():
+    fakes = [FakeTransport(latency_s=0.01) for _ in range(4)]
+    s = scheduler(fakes, target_photons_per_batch=100, max_events_per_batch=1, batch_collection_timeout_ms=1)
+    futures = [s.submit(event(e)) for e in range(16)]
+    for e, f in enumerate(futures):
+        assert f.result(timeout=30).event_statistics[0][0] == e
+    s.end_run()
+    assert all(len(f.batches) >= 2 for f in fakes)
+    assert s.batch_statistics()["overlapped_batch_count"] >= 8
+    s.close()
