@@ -554,8 +554,11 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
     FlushRunCounters(p, tally.bounces, coincidentTraces, coincidentHits, lane);
 }
 
+// Two resident 256-thread blocks per SM (at most 128 registers): for the
+// FP64 form this measured 6 % faster than the compiler's unconstrained
+// allocation of 173 registers, despite a few spills.
 template<class R, bool kDiagnostics>
-__global__ void __launch_bounds__(256) TransportPlain(const LaunchParams p) {
+__global__ void __launch_bounds__(256, 2) TransportPlain(const LaunchParams p) {
     LoadScene(p);
     const PackedScene& scene{*reinterpret_cast<const PackedScene*>(gShared)};
     const float* pool{PoolOf(scene)};
