@@ -494,16 +494,17 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
             queueHead += min(static_cast<std::uint32_t>(__popc(need)), available);
             need = __ballot_sync(kFullMask, !alive);
         }
+        // no photon to step and no fresh work left: complete what is pending,
+        // even if fewer than 32, at the one completion site below
+        bool draining{false};
         if (__ballot_sync(kFullMask, alive) == 0U) {
-            if (pendingEnd != pendingHead) {
-                // no fresh work left: complete what is pending, even if fewer than 32
-                ResolvePending(ring, pendingHead, min(pendingEnd - pendingHead, 32U), lane, p, epsilon);
-                continue;
+            if (pendingEnd == pendingHead) {
+                if (pendingHead != readyHead) {
+                    continue;
+                }
+                break;
             }
-            if (pendingHead != readyHead) {
-                continue;
-            }
-            break;
+            draining = true;
         }
 
         std::uint32_t result{kContinue};
@@ -546,8 +547,9 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
             }
         }
         __syncwarp();
-        if (pendingEnd - pendingHead >= 32U) {
-            ResolvePending(ring, pendingHead, 32U, lane, p, epsilon);
+        const std::uint32_t pending{pendingEnd - pendingHead};
+        if (pending >= 32U || (draining && pending != 0U)) {
+            ResolvePending(ring, pendingHead, min(pending, 32U), lane, p, epsilon);
         }
     }
     counters.Flush(p.events);
