@@ -14,15 +14,21 @@
 // The batch type is generic: anything with `emissions`, `eventIDs` and
 // `emissionEventIndices` spans whose element is the 128-byte OpticalEmission
 // record (PhotonTransport.hpp:159-163) is passed through without copying.
+// The scene is either a g4b_scene of boxes or the reference's exported Scene
+// itself, converted by g4b::BoxScene (g4b_scene_adapter.hpp).
 #pragma once
 
 #include <cstddef>
 #include <cstdint>
+#include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "g4b.h"
+#include "g4b_scene_adapter.hpp"
 
 namespace g4b {
 
@@ -69,8 +75,21 @@ public:
         fSceneAddress = &scene;
     }
 
-    template<class Batch>
-    void EnqueueEmissions(const g4b_scene& scene, const Batch& batch) {
+    // The reference's own Scene (meshes + transforms): converted to boxes by
+    // g4b::BoxScene, again only when a scene at a different address is passed.
+    template<class Scene, class = decltype(std::declval<const Scene&>().Volumes())>
+    void PrepareScene(const Scene& scene) {
+        if (fSceneAddress == static_cast<const void*>(&scene)) {
+            return;
+        }
+        auto boxes{std::make_unique<BoxScene>(scene)};
+        Check(g4b_set_scene(fHandle, &boxes->Get()));
+        fBoxScene = std::move(boxes);
+        fSceneAddress = &scene;
+    }
+
+    template<class Scene, class Batch>
+    void EnqueueEmissions(const Scene& scene, const Batch& batch) {
         static_assert(sizeof(*batch.emissions.data()) == sizeof(g4b_optical_emission),
                       "emission records must be the 128-byte OpticalEmission layout");
         PrepareScene(scene);
@@ -116,7 +135,8 @@ private:
     }
 
     g4b_handle* fHandle{nullptr};
-    const g4b_scene* fSceneAddress{nullptr};
+    const void* fSceneAddress{nullptr};
+    std::unique_ptr<BoxScene> fBoxScene;
 };
 
 }  // namespace g4b
