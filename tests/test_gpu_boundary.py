@@ -2,8 +2,9 @@
 
 Boundary physics against the reference's own outputs (golden vectors made by
 tests/golden/make_golden.py from the reference's OptiXBoundaryPhysics.cuh)
-and the reference's known-answer tests, at the north_star tolerance of 1e-5;
-the device math and RNG bit for bit against the CPU oracle.
+and the reference's known-answer tests, within 1e-5 relative (the agreement
+with the Geant4 formulas that is required); the device math and RNG bit for bit
+against the CPU oracle.
 """
 import ctypes as C
 import math

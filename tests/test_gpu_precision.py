@@ -4,7 +4,7 @@
   380-500 nm, through the FP32 and FP64 engines with the same RNG counters:
   per-photon fate agreement and arrival-time error of the FP32 form against
   the FP64 one.
-- Equal accuracy (north_star): the batched FP32 engine against the FP64 CPU
+- Equal accuracy: the batched FP32 engine against the FP64 CPU
   oracle run with an independent seed on the same gensteps: mean detected
   count within 0.5 % and a two-sample KS test on arrival times with p > 0.01.
 - Full-size invariants: photon conservation, per-event sums, hit counts,

@@ -170,7 +170,7 @@ def test_oracle_fresnel_matches_reference_golden(oracle, precision):
           golden["fresnel_index_from"][i], golden["fresnel_index_to"][i])
         for i in range(golden["fresnel_direction"].shape[0])
     ], dtype=np.float64)
-    # north_star tolerance for the boundary unit cases: 1e-5
+    # required agreement of the boundary unit cases with the formulas: 1e-5 relative
     _fresnel_golden_check(rows, golden, tolerance=1e-5)
 
 
