@@ -117,7 +117,8 @@ class Config(C.Structure):
         ("chunk_photons", C.c_uint32),
         ("use_cuda_graph", C.c_uint32),
         ("record_photon_fates", C.c_uint32),
-        ("reserved", C.c_uint32 * 7),
+        ("generation_pass", C.c_uint32),
+        ("reserved", C.c_uint32 * 6),
     ]
 
 

@@ -170,6 +170,12 @@ struct g4b_handle {
     DeviceBuffer dHits[kHitColumns];
     std::uint64_t hitCapacity{0};
     DeviceBuffer dBitmap, dPrefix, dBlockSums, dDetections, dFate, dFateTime, dGradient;
+    DeviceBuffer dStore;    // two photon stores of the generation pass (waves alternate)
+    DeviceBuffer dTickets;  // the two waves' device work tickets
+    cudaStream_t generationStream{nullptr};
+    cudaEvent_t zeroedEvent{nullptr};
+    cudaEvent_t generatedEvent[2]{};
+    cudaEvent_t storeFreeEvent[2]{};
 
     // The staged batch (kept for g4b_relaunch) and the pending one.
     bool hasStaged{false};
@@ -214,10 +220,18 @@ namespace {
 int Precision(const g4b_handle& h) { return h.config.precision == G4B_PRECISION_FP64 ? g4b::kFP64 : g4b::kFP32; }
 int Form(const g4b_handle& h) { return h.config.launch_form == G4B_FORM_PLAIN ? g4b::kPlain : g4b::kBatched; }
 
+// The batched FP32 form makes its photons in a separate generation pass
+// unless the configuration asks for generation inside the transport loop.
+bool UsesGenerationPass(const g4b_handle& h) {
+    return Form(h) == g4b::kBatched && Precision(h) == g4b::kFP32 && h.config.generation_pass != 2U;
+}
+
 // The kernel variant of a form: with the coincidence counters only when
-// performance diagnostics are enabled, as the reference counts them.
+// performance diagnostics are enabled, as the reference counts them, and for
+// the batched form with a generation pass the one that reads the photon store.
 int KernelOf(const g4b_handle& h, int form) {
-    return form | (h.config.enable_performance_diagnostics != 0 ? g4b::kWithDiagnostics : 0);
+    return form | (h.config.enable_performance_diagnostics != 0 ? g4b::kWithDiagnostics : 0) |
+           (form == g4b::kBatched && UsesGenerationPass(h) ? g4b::kPregenerated : 0);
 }
 
 std::size_t SceneSharedBytes(const g4b_handle& h) {
@@ -225,12 +239,13 @@ std::size_t SceneSharedBytes(const g4b_handle& h) {
 }
 
 // Dynamic shared memory of a launch: the scene blob, plus one photon queue
-// and one Fresnel ring per warp for the batched form.
+// (not with a generation pass) and one Fresnel ring per warp and one tally
+// per lane for the batched form.
 std::size_t SharedBytes(const g4b_handle& h, int form, std::uint32_t blockSize) {
     std::size_t bytes{SceneSharedBytes(h)};
     if (form == g4b::kBatched) {
         const bool fp64{h.config.precision == G4B_PRECISION_FP64};
-        const std::size_t queue{fp64 ? g4b::kQueueBytesFP64 : g4b::kQueueBytesFP32};
+        const std::size_t queue{UsesGenerationPass(h) ? 0U : (fp64 ? g4b::kQueueBytesFP64 : g4b::kQueueBytesFP32)};
         const std::size_t ring{fp64 ? g4b::kRingBytesFP64 : g4b::kRingBytesFP32};
         bytes += (queue + ring) * (blockSize / 32U) + g4b::kLaneTallyBytes * blockSize;
     }
@@ -238,6 +253,7 @@ std::size_t SharedBytes(const g4b_handle& h, int form, std::uint32_t blockSize) 
 }
 
 std::uint32_t RoundChunk(std::uint32_t chunk) { return std::max<std::uint32_t>((chunk + 31U) / 32U * 32U, 32U); }
+
 
 // --- scene packing ---------------------------------------------------------
 
@@ -591,6 +607,7 @@ LaunchParams BaseParams(const g4b_handle& h) {
     p.epsilon = h.config.boundary_tolerance_mm;
     p.events = h.dEvents.As<EventCounters>();
     p.run = h.dRun.As<RunCounters>();
+    p.workTicket = &p.run->workTicket;
     HitColumns hits{};
     hits.positionX = h.dHits[0].As<float>();
     hits.positionY = h.dHits[1].As<float>();
@@ -684,6 +701,112 @@ void LaunchBatchedGraph(g4b_handle& h, const LaunchParams& params, unsigned grid
     Check(cudaGraphLaunch(h.graphExec, h.stream), "cudaGraphLaunch");
 }
 
+// Photons per wave of the generation pass: the batch cut into equal waves
+// of at most kPhotonStoreWave.
+std::uint64_t WavePhotons(const g4b_handle& h) {
+    const std::uint64_t waves{(h.photonCount + g4b::kPhotonStoreWave - 1U) / g4b::kPhotonStoreWave};
+    return waves == 0U ? 0U : (h.photonCount + waves - 1U) / waves;
+}
+
+// Bytes of one photon store for `rows` photons: 256-byte aligned columns.
+std::size_t StoreBytes(std::uint64_t rows) {
+    const auto rounded{[](std::size_t bytes) { return (bytes + 255U) & ~std::size_t{255}; }};
+    return 10U * rounded(rows * sizeof(float)) + rounded(rows * sizeof(double)) +
+           4U * rounded(rows * sizeof(std::uint32_t));
+}
+
+// Column views of photon store `which` (0 or 1) of the handle's allocation,
+// each store sized for `rows` photons.
+g4b::PhotonStore StoreView(g4b_handle& h, std::uint64_t rows, int which) {
+    const auto rounded{[](std::size_t bytes) { return (bytes + 255U) & ~std::size_t{255}; }};
+    const std::size_t floatColumn{rounded(rows * sizeof(float))};
+    const std::size_t doubleColumn{rounded(rows * sizeof(double))};
+    const std::size_t wordColumn{rounded(rows * sizeof(std::uint32_t))};
+    char* next{h.dStore.As<char>() + static_cast<std::size_t>(which) * StoreBytes(rows)};
+    const auto column{[&](std::size_t bytes) {
+        char* start{next};
+        next += bytes;
+        return start;
+    }};
+    g4b::PhotonStore store{};
+    for (int axis{}; axis < 3; ++axis) {
+        store.position[axis] = reinterpret_cast<float*>(column(floatColumn));
+        store.direction[axis] = reinterpret_cast<float*>(column(floatColumn));
+        store.polarization[axis] = reinterpret_cast<float*>(column(floatColumn));
+    }
+    store.energy = reinterpret_cast<float*>(column(floatColumn));
+    store.time = reinterpret_cast<double*>(column(doubleColumn));
+    store.eventID = reinterpret_cast<std::uint32_t*>(column(wordColumn));
+    store.photonID = reinterpret_cast<std::uint32_t*>(column(wordColumn));
+    store.volume = reinterpret_cast<std::uint32_t*>(column(wordColumn));
+    store.eventIndex = reinterpret_cast<std::uint32_t*>(column(wordColumn));
+    return store;
+}
+
+void EnsureGenerationStream(g4b_handle& h) {
+    if (h.generationStream != nullptr) {
+        return;
+    }
+    Check(cudaStreamCreateWithFlags(&h.generationStream, cudaStreamNonBlocking), "cudaStreamCreateWithFlags");
+    Check(cudaEventCreateWithFlags(&h.zeroedEvent, cudaEventDisableTiming), "cudaEventCreate");
+    for (int k{}; k < 2; ++k) {
+        Check(cudaEventCreateWithFlags(&h.generatedEvent[k], cudaEventDisableTiming), "cudaEventCreate");
+        Check(cudaEventCreateWithFlags(&h.storeFreeEvent[k], cudaEventDisableTiming), "cudaEventCreate");
+    }
+}
+
+// Batched FP32 form with a generation pass. The batch is cut into equal waves
+// of at most kPhotonStoreWave photons. GeneratePhotons fills a wave's store
+// on the generation stream, and the transport kernel then takes the wave's
+// photons from it on the handle's stream. The two stores and work tickets
+// alternate, so wave k+1 is generated while wave k is transported: its blocks
+// fill the SMs that wave k's finished warps leave. Counters are zeroed once
+// per batch. Returns the number of kernels launched.
+std::uint64_t LaunchBatchedWaves(g4b_handle& h, const LaunchParams& base, unsigned grid, std::uint32_t block) {
+    EnsureGenerationStream(h);
+    const std::uint64_t wave{WavePhotons(h)};
+    const std::uint64_t waves{(h.photonCount + wave - 1U) / wave};
+    h.dStore.Ensure(2U * StoreBytes(wave), "cudaMalloc photon stores");
+    h.dTickets.Ensure(2U * sizeof(unsigned int), "cudaMalloc work tickets");
+    const auto waveParams{[&](std::uint64_t k) {
+        LaunchParams p{base};
+        p.photonBegin = static_cast<std::uint32_t>(k * wave);
+        p.photonEnd = static_cast<std::uint32_t>(std::min<std::uint64_t>((k + 1U) * wave, h.photonCount));
+        p.store = StoreView(h, wave, static_cast<int>(k % 2U));
+        p.workTicket = h.dTickets.As<unsigned int>() + k % 2U;
+        return p;
+    }};
+    const unsigned generateGrid{static_cast<unsigned>(h.smCount) * 8U};
+    Check(g4b::LaunchZeroCounters(base.events, base.eventCount, base.run, h.stream), "zero counters");
+    Check(cudaEventRecord(h.zeroedEvent, h.stream), "cudaEventRecord");
+    Check(cudaStreamWaitEvent(h.generationStream, h.zeroedEvent, 0), "cudaStreamWaitEvent");
+    Check(g4b::LaunchGenerate(waveParams(0), generateGrid, SceneSharedBytes(h), h.generationStream),
+          "generation launch");
+    Check(cudaEventRecord(h.generatedEvent[0], h.generationStream), "cudaEventRecord");
+    std::uint64_t launches{2};
+    for (std::uint64_t k{0}; k < waves; ++k) {
+        const LaunchParams p{waveParams(k)};
+        Check(cudaStreamWaitEvent(h.stream, h.generatedEvent[k % 2U], 0), "cudaStreamWaitEvent");
+        Check(cudaMemsetAsync(p.workTicket, 0, sizeof(unsigned int), h.stream), "reset work ticket");
+        Check(g4b::LaunchTransport(p, g4b::kFP32, KernelOf(h, g4b::kBatched) | g4b::kPregenerated, grid, block,
+                                   SharedBytes(h, g4b::kBatched, block), h.stream),
+              "transport launch");
+        Check(cudaEventRecord(h.storeFreeEvent[k % 2U], h.stream), "cudaEventRecord");
+        ++launches;
+        if (k + 1U < waves) {
+            if (k >= 1U) {  // the next wave's store and ticket were last used by wave k - 1
+                Check(cudaStreamWaitEvent(h.generationStream, h.storeFreeEvent[(k + 1U) % 2U], 0),
+                      "cudaStreamWaitEvent");
+            }
+            Check(g4b::LaunchGenerate(waveParams(k + 1U), generateGrid, SceneSharedBytes(h), h.generationStream),
+                  "generation launch");
+            Check(cudaEventRecord(h.generatedEvent[(k + 1U) % 2U], h.generationStream), "cudaEventRecord");
+            ++launches;
+        }
+    }
+    return launches;
+}
+
 // Hit rows reserved by default: a quarter of the photons (at least 2^20, at
 // most all of them). Overflow is caught after the launch and the batch is
 // rerun with an exact-size buffer, which gives identical results because
@@ -704,18 +827,22 @@ void RunStaged(g4b_handle& h) {
             // photons (and its tail) are shared out over every warp; never
             // more than the configured chunk
             const std::uint64_t warps{static_cast<std::uint64_t>(grid) * (h.blockSize / 32U)};
-            const std::uint64_t perWarp{h.photonCount / (warps * 8U)};
+            const std::uint64_t photons{UsesGenerationPass(h) ? WavePhotons(h) : h.photonCount};
+            const std::uint64_t perWarp{photons / (warps * 8U)};
             base.chunk = RoundChunk(static_cast<std::uint32_t>(std::clamp<std::uint64_t>(perWarp, 32U, h.chunk)));
         }
-        if (h.config.use_cuda_graph != 0) {
+        if (UsesGenerationPass(h)) {
+            h.launchCount += LaunchBatchedWaves(h, base, grid, h.blockSize);
+        } else if (h.config.use_cuda_graph != 0) {
             LaunchBatchedGraph(h, base, grid);
+            h.launchCount += 2;
         } else {
             Check(g4b::LaunchZeroCounters(base.events, base.eventCount, base.run, h.stream), "zero counters");
             Check(g4b::LaunchTransport(base, Precision(h), KernelOf(h, g4b::kBatched), grid, h.blockSize,
                                        SharedBytes(h, g4b::kBatched, h.blockSize), h.stream),
                   "transport launch");
+            h.launchCount += 2;
         }
-        h.launchCount += 2;
     } else {
         Check(g4b::LaunchZeroCounters(base.events, base.eventCount, base.run, h.stream), "zero counters");
         ++h.launchCount;
@@ -1188,6 +1315,9 @@ int g4b_destroy(g4b_handle* handle) {
     if (handle->stream != nullptr) {
         cudaStreamSynchronize(handle->stream);
     }
+    if (handle->generationStream != nullptr) {
+        cudaStreamSynchronize(handle->generationStream);
+    }
     DestroyGraph(*handle);
     handle->hostToDeviceTimer.Destroy();
     handle->memsetTimer.Destroy();
@@ -1196,6 +1326,15 @@ int g4b_destroy(g4b_handle* handle) {
     handle->hitsTimer.Destroy();
     if (handle->metadataReadyEvent != nullptr) {
         cudaEventDestroy(handle->metadataReadyEvent);
+    }
+    for (cudaEvent_t event : {handle->zeroedEvent, handle->generatedEvent[0], handle->generatedEvent[1],
+                              handle->storeFreeEvent[0], handle->storeFreeEvent[1]}) {
+        if (event != nullptr) {
+            cudaEventDestroy(event);
+        }
+    }
+    if (handle->generationStream != nullptr) {
+        cudaStreamDestroy(handle->generationStream);
     }
     if (handle->stream != nullptr) {
         cudaStreamDestroy(handle->stream);
@@ -1415,14 +1554,20 @@ int g4b_autotune(g4b_handle* h, const uint32_t* blockSizes, uint32_t nBlockSizes
                     const unsigned grid{static_cast<unsigned>(h->smCount) * blocksPerSM};
                     double total{0.0};
                     for (std::uint32_t r{}; r < repeats + 1; ++r) {
-                        Check(g4b::LaunchZeroCounters(p.events, p.eventCount, p.run, h->stream), "zero counters");
-                        Check(cudaEventRecord(h->kernelTimer.start, h->stream), "cudaEventRecord");
-                        Check(g4b::LaunchTransport(p, Precision(*h), KernelOf(*h, g4b::kBatched), grid, block,
-                                                   SharedBytes(*h, g4b::kBatched, block), h->stream),
-                              "transport launch");
+                        if (UsesGenerationPass(*h)) {
+                            Check(cudaEventRecord(h->kernelTimer.start, h->stream), "cudaEventRecord");
+                            h->launchCount += LaunchBatchedWaves(*h, p, grid, block);
+                        } else {
+                            Check(g4b::LaunchZeroCounters(p.events, p.eventCount, p.run, h->stream),
+                                  "zero counters");
+                            Check(cudaEventRecord(h->kernelTimer.start, h->stream), "cudaEventRecord");
+                            Check(g4b::LaunchTransport(p, Precision(*h), KernelOf(*h, g4b::kBatched), grid, block,
+                                                       SharedBytes(*h, g4b::kBatched, block), h->stream),
+                                  "transport launch");
+                            h->launchCount += 2;
+                        }
                         Check(cudaEventRecord(h->kernelTimer.stop, h->stream), "cudaEventRecord");
                         Check(cudaEventSynchronize(h->kernelTimer.stop), "cudaEventSynchronize");
-                        h->launchCount += 2;
                         if (r > 0) {
                             total += h->kernelTimer.Milliseconds();
                         }

@@ -160,6 +160,23 @@ struct HitColumns {
     unsigned long long capacity;
 };
 
+// Photons of one wave of the batched FP32 form, made by the generation pass
+// and read by the transport: one column per field, row = slot - photonBegin.
+// eventIndex == kInvalidID marks a photon that failed the validity test.
+struct PhotonStore {
+    float* position[3];
+    float* direction[3];
+    float* polarization[3];
+    float* energy;
+    double* time;
+    std::uint32_t* eventID;
+    std::uint32_t* photonID;
+    std::uint32_t* volume;
+    std::uint32_t* eventIndex;
+};
+constexpr std::uint32_t kPhotonStoreBytes{10U * 4U + 8U + 4U * 4U};  // per photon: 64
+constexpr std::uint32_t kPhotonStoreWave{1U << 26};                  // most photons in one generation wave
+
 struct LaunchParams {
     const float4* emissions;               // [emissionCount] 128-byte gensteps as 8 float4 each
     const std::uint32_t* emissionOffsets;  // [emissionCount + 1] exclusive prefix of photon counts
@@ -183,6 +200,8 @@ struct LaunchParams {
     HitColumns hits;
     std::uint32_t* photonFate;             // optional [photons]
     double* photonTime;                    // optional [photons]
+    PhotonStore store;                     // batched FP32 form with a generation pass
+    unsigned int* workTicket;              // batched form: next unclaimed photon of the launch
 };
 
 }  // namespace g4b

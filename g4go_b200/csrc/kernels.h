@@ -11,12 +11,15 @@
 namespace g4b {
 
 enum KernelPrecision : int { kFP32 = 0, kFP64 = 1 };
-enum KernelForm : int { kBatched = 0, kPlain = 1, kWithDiagnostics = 2 };
+enum KernelForm : int { kBatched = 0, kPlain = 1, kWithDiagnostics = 2, kPregenerated = 4 };
 
 // The transport kernel for (precision, form), as a function pointer usable in
 // cudaLaunchKernel and in graph kernel nodes. `form` may carry
-// kWithDiagnostics: the variant that also counts coincident-face retraces.
+// kWithDiagnostics (the variant that also counts coincident-face retraces)
+// and, for the batched FP32 form, kPregenerated (photons read from the
+// photon store instead of generated in the loop).
 const void* TransportKernel(int precision, int form);
+const void* GenerateKernel();
 const void* ZeroCountersKernel();
 
 // Raises the dynamic shared-memory limit of every transport kernel.
@@ -28,6 +31,11 @@ cudaError_t LaunchZeroCounters(EventCounters* events, std::uint32_t eventCount, 
 
 cudaError_t LaunchTransport(const LaunchParams& params, int precision, int form, unsigned grid, unsigned block,
                             std::size_t sharedBytes, cudaStream_t stream);
+
+// Generation pass of the batched FP32 form: fills params.store with the
+// photons [photonBegin, photonEnd) (256-thread blocks, the scene in shared
+// memory).
+cudaError_t LaunchGenerate(const LaunchParams& params, unsigned grid, std::size_t sharedBytes, cudaStream_t stream);
 
 // Ordered compaction: orders `count` hits by their flattened-photon slot
 // (the order cub::DeviceSelect::Flagged gives the reference,

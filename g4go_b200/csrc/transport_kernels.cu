@@ -182,6 +182,87 @@ __device__ __forceinline__ void RecordFate(const LaunchParams& p, std::uint32_t 
     }
 }
 
+// Row i of the photon store: a generated, valid FP32 photon.
+__device__ __forceinline__ void StorePhoton(const PhotonStore& store, std::uint32_t i, const Photon<float>& photon) {
+    store.position[0][i] = photon.position.x;
+    store.position[1][i] = photon.position.y;
+    store.position[2][i] = photon.position.z;
+    store.direction[0][i] = photon.direction.x;
+    store.direction[1][i] = photon.direction.y;
+    store.direction[2][i] = photon.direction.z;
+    store.polarization[0][i] = photon.polarization.x;
+    store.polarization[1][i] = photon.polarization.y;
+    store.polarization[2][i] = photon.polarization.z;
+    store.energy[i] = photon.energy;
+    store.time[i] = photon.time;
+    store.eventID[i] = photon.eventID;
+    store.photonID[i] = photon.photonID;
+    store.volume[i] = photon.volume;
+    store.eventIndex[i] = photon.eventIndex;
+}
+
+// Reads row i back; false for a photon that failed the validity test.
+__device__ __forceinline__ bool LoadStoredPhoton(const PhotonStore& store, std::uint32_t i, std::uint32_t slot,
+                                                 Photon<float>& photon) {
+    photon.eventIndex = __ldcs(store.eventIndex + i);
+    if (photon.eventIndex == kInvalidID) {
+        return false;
+    }
+    photon.position = {__ldcs(store.position[0] + i), __ldcs(store.position[1] + i), __ldcs(store.position[2] + i)};
+    photon.direction = {__ldcs(store.direction[0] + i), __ldcs(store.direction[1] + i),
+                        __ldcs(store.direction[2] + i)};
+    photon.polarization = {__ldcs(store.polarization[0] + i), __ldcs(store.polarization[1] + i),
+                           __ldcs(store.polarization[2] + i)};
+    photon.energy = __ldcs(store.energy + i);
+    photon.time = __ldcs(store.time + i);
+    photon.eventID = __ldcs(store.eventID + i);
+    photon.photonID = __ldcs(store.photonID + i);
+    photon.volume = __ldcs(store.volume + i);
+    photon.slot = slot;
+    photon.bounce = 0U;
+    return true;
+}
+
+// Generation pass of the batched FP32 form: every photon of the wave
+// [photonBegin, photonEnd) made from its genstep and RNG counters as the
+// transport kernel would make it, validity-tested (invalid ones counted and
+// recorded here) and written to the store. A warp takes 32 consecutive slots:
+// one binary search for the first, a forward scan per lane.
+__global__ void __launch_bounds__(256) GeneratePhotons(const LaunchParams p) {
+    LoadScene(p);
+    const PackedScene& scene{*reinterpret_cast<const PackedScene*>(gShared)};
+    const float* pool{PoolOf(scene)};
+    const unsigned lane{threadIdx.x & 31U};
+    const std::uint32_t warps{gridDim.x * (blockDim.x >> 5U)};
+    const std::uint32_t warp{blockIdx.x * (blockDim.x >> 5U) + (threadIdx.x >> 5U)};
+    for (std::uint32_t base{p.photonBegin + warp * 32U}; base < p.photonEnd; base += warps * 32U) {
+        const std::uint32_t slot{base + lane};
+        if (slot >= p.photonEnd) {
+            continue;
+        }
+        std::uint32_t e{FindEmission(p.emissionOffsets, p.emissionBegin, p.emissionEnd, base)};
+        while (__ldg(p.emissionOffsets + e + 1U) <= slot) {
+            ++e;
+        }
+        Emission emission;
+        LoadEmission(p.emissions, e, emission);
+        const std::uint32_t local{slot - __ldg(p.emissionOffsets + e)};
+        const std::uint32_t eventIndex{__ldg(p.emissionEventIndices + e)};
+        Photon<float> photon{};
+        GeneratePhoton<float>(scene, pool, emission, emission.FirstPhotonID() + local, p.seed, NoGradient(), photon);
+        photon.eventIndex = eventIndex;
+        photon.slot = slot;
+        const std::uint32_t row{slot - p.photonBegin};
+        if (StartPhoton(photon)) {
+            StorePhoton(p.store, row, photon);
+        } else {
+            atomicAdd(&p.events[eventIndex].invalid, 1ULL);
+            RecordFate(p, slot, kInvalid, 0U, photon.time);
+            p.store.eventIndex[row] = kInvalidID;
+        }
+    }
+}
+
 // The shared-memory photon queue of one warp (layout sizes kQueueBytesFP32/64).
 template<class R>
 struct WarpQueue {
@@ -360,7 +441,9 @@ struct BatchedMinBlocks<double> {
 // kDiagnostics: count coincident-face retraces and hits, which the reference
 // does only with enablePerformanceDiagnostics (OptiXTransportDevice.cu:752-775);
 // without it the counting is compiled out, which frees registers in the loop.
-template<class R, bool kDiagnostics>
+// kPregenerated (FP32 only): the wave's photons come from the photon store
+// that GeneratePhotons filled, and the loop carries no generation code.
+template<class R, bool kDiagnostics, bool kPregenerated = false>
 __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatched(const LaunchParams p) {
     LoadScene(p);
     const PackedScene& scene{*reinterpret_cast<const PackedScene*>(gShared)};
@@ -370,13 +453,15 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
     const R epsilon{R(p.epsilon)};
     const std::uint32_t totalPhotons{p.photonEnd - p.photonBegin};
     const std::uint32_t sceneEnd{(p.sceneBytes + 15U) & ~15U};
-    WarpQueue<R>& queue{
-        *reinterpret_cast<WarpQueue<R>*>(gShared + sceneEnd + (threadIdx.x >> 5U) * sizeof(WarpQueue<R>))};
+    // shared memory: scene, then one photon queue per warp (not with
+    // kPregenerated: lanes take photons straight from the store), one Fresnel
+    // ring per warp, one tally per lane
     const std::uint32_t warps{blockDim.x >> 5U};
-    FresnelRing<R>& ring{*reinterpret_cast<FresnelRing<R>*>(gShared + sceneEnd + warps * sizeof(WarpQueue<R>) +
+    constexpr std::uint32_t kQueueBytes{kPregenerated ? 0U : static_cast<std::uint32_t>(sizeof(WarpQueue<R>))};
+    WarpQueue<R>& queue{*reinterpret_cast<WarpQueue<R>*>(gShared + sceneEnd + (threadIdx.x >> 5U) * kQueueBytes)};
+    FresnelRing<R>& ring{*reinterpret_cast<FresnelRing<R>*>(gShared + sceneEnd + warps * kQueueBytes +
                                                             (threadIdx.x >> 5U) * sizeof(FresnelRing<R>))};
-    LaneTally& tally{*reinterpret_cast<LaneTally*>(gShared + sceneEnd +
-                                                   warps * (sizeof(WarpQueue<R>) + sizeof(FresnelRing<R>)) +
+    LaneTally& tally{*reinterpret_cast<LaneTally*>(gShared + sceneEnd + warps * (kQueueBytes + sizeof(FresnelRing<R>)) +
                                                    threadIdx.x * sizeof(LaneTally))};
     constexpr std::uint32_t kRing{FresnelRing<R>::kEntries};
     std::uint32_t readyHead{0U};
@@ -428,6 +513,41 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
             __syncwarp();
             need = __ballot_sync(kFullMask, !alive);
         }
+        if constexpr (kPregenerated) {
+            // Lanes that need a photon take the next slots of the warp's chunk
+            // straight from the store; a photon that failed the validity test
+            // leaves its lane needing one.
+            while (need != 0U) {
+                if (chunkNext >= chunkEnd) {
+                    if (workDone) {
+                        break;
+                    }
+                    std::uint32_t start{0U};
+                    if (lane == 0U) {
+                        start = atomicAdd(p.workTicket, p.chunk);
+                    }
+                    start = __shfl_sync(kFullMask, start, 0);
+                    if (start >= totalPhotons) {
+                        workDone = true;
+                        break;
+                    }
+                    chunkNext = p.photonBegin + start;
+                    chunkEnd = p.photonBegin + min(start + p.chunk, totalPhotons);
+                }
+                const std::uint32_t available{chunkEnd - chunkNext};
+                const std::uint32_t rank{static_cast<std::uint32_t>(__popc(need & lanesBelow))};
+                if (((need >> lane) & 1U) != 0U && rank < available) {
+                    const std::uint32_t slot{chunkNext + rank};
+                    if (LoadStoredPhoton(p.store, slot - p.photonBegin, slot, photon)) {
+                        counters.Switch(photon.eventIndex, p.events);
+                        alive = true;
+                    }
+                }
+                chunkNext += min(static_cast<std::uint32_t>(__popc(need)), available);
+                need = __ballot_sync(kFullMask, !alive);
+            }
+        }
+        if constexpr (!kPregenerated) {
         while (need != 0U) {
             if (queueHead == queueCount) {
                 if (workDone) {
@@ -437,7 +557,7 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
                 if (chunkNext >= chunkEnd) {
                     std::uint32_t start{0U};
                     if (lane == 0U) {
-                        start = atomicAdd(&p.run->workTicket, p.chunk);
+                        start = atomicAdd(p.workTicket, p.chunk);
                     }
                     start = __shfl_sync(kFullMask, start, 0);
                     if (start >= totalPhotons) {
@@ -462,7 +582,8 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
                     LoadEmission(p.emissions, e, emission);
                     const std::uint32_t local{slot - __ldg(p.emissionOffsets + e)};
                     const std::uint32_t eventIndex{__ldg(p.emissionEventIndices + e)};
-                    GeneratePhoton<R>(scene, pool, emission, emission.FirstPhotonID() + local, p.seed, NoGradient(), fresh);
+                    GeneratePhoton<R>(scene, pool, emission, emission.FirstPhotonID() + local, p.seed, NoGradient(),
+                                      fresh);
                     fresh.eventIndex = eventIndex;
                     fresh.slot = (p.slotBase != nullptr) ? __ldg(p.slotBase + e) + local : slot;
                     valid = StartPhoton(fresh);
@@ -493,6 +614,7 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
             }
             queueHead += min(static_cast<std::uint32_t>(__popc(need)), available);
             need = __ballot_sync(kFullMask, !alive);
+        }
         }
         // no photon to step and no fresh work left: complete what is pending,
         // even if fewer than 32, at the one completion site below
@@ -1047,15 +1169,24 @@ const void* TransportKernel(int precision, int form) {
         return diagnostics ? reinterpret_cast<const void*>(&TransportBatched<double, true>)
                            : reinterpret_cast<const void*>(&TransportBatched<double, false>);
     }
+    if ((form & kPregenerated) != 0) {
+        return diagnostics ? reinterpret_cast<const void*>(&TransportBatched<float, true, true>)
+                           : reinterpret_cast<const void*>(&TransportBatched<float, false, true>);
+    }
     return diagnostics ? reinterpret_cast<const void*>(&TransportBatched<float, true>)
                        : reinterpret_cast<const void*>(&TransportBatched<float, false>);
 }
+
+const void* GenerateKernel() { return reinterpret_cast<const void*>(&GeneratePhotons); }
 
 const void* ZeroCountersKernel() { return reinterpret_cast<const void*>(&ZeroCounters); }
 
 cudaError_t ConfigureTransportKernels(std::size_t sharedBytes) {
     for (int precision = 0; precision < 2; ++precision) {
-        for (int form = 0; form < 4; ++form) {  // kBatched, kPlain, each with and without kWithDiagnostics
+        // kBatched, kPlain, each with and without kWithDiagnostics, and the
+        // pregenerated batched kernels (FP32)
+        constexpr int kForms[]{0, 1, 2, 3, 4, 6};
+        for (const int form : kForms) {
             const cudaError_t error{cudaFuncSetAttribute(TransportKernel(precision, form),
                                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                          static_cast<int>(sharedBytes))};
@@ -1064,7 +1195,8 @@ cudaError_t ConfigureTransportKernels(std::size_t sharedBytes) {
             }
         }
     }
-    return cudaSuccess;
+    return cudaFuncSetAttribute(GenerateKernel(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(sharedBytes));
 }
 
 cudaError_t TransportOccupancy(int precision, int form, int blockSize, std::size_t sharedBytes, int* blocksPerSM) {
@@ -1076,6 +1208,11 @@ cudaError_t LaunchZeroCounters(EventCounters* events, std::uint32_t eventCount, 
                                cudaStream_t stream) {
     const unsigned long long words{static_cast<unsigned long long>(eventCount) * (sizeof(EventCounters) / 16U)};
     ZeroCounters<<<BlocksFor(words < 32ULL ? 32ULL : words, 256U), 256, 0, stream>>>(events, eventCount, run);
+    return cudaGetLastError();
+}
+
+cudaError_t LaunchGenerate(const LaunchParams& params, unsigned grid, std::size_t sharedBytes, cudaStream_t stream) {
+    GeneratePhotons<<<grid, 256, sharedBytes, stream>>>(params);
     return cudaGetLastError();
 }
 

@@ -257,6 +257,7 @@ class PhotonTransportConfig:
     chunk_photons: int = 0
     use_cuda_graph: bool = True
     record_photon_fates: bool = False
+    generation_pass: int = 0  # batched FP32: 0/1 separate generation kernel, 2 generation inside the loop
     device: int = -1
 
     def to_c(self) -> _abi.Config:
@@ -280,6 +281,7 @@ class PhotonTransportConfig:
         config.chunk_photons = int(self.chunk_photons)
         config.use_cuda_graph = int(bool(self.use_cuda_graph))
         config.record_photon_fates = int(bool(self.record_photon_fates))
+        config.generation_pass = int(self.generation_pass)
         return config
 
 
