@@ -176,6 +176,7 @@ struct g4b_handle {
     cudaEvent_t zeroedEvent{nullptr};
     cudaEvent_t generatedEvent[2]{};
     cudaEvent_t storeFreeEvent[2]{};
+    cudaGraphExec_t wavesExec{nullptr};  // the generation-pass waves of the last batch, captured
 
     // The staged batch (kept for g4b_relaunch) and the pending one.
     bool hasStaged{false};
@@ -762,12 +763,16 @@ void EnsureGenerationStream(g4b_handle& h) {
 // alternate, so wave k+1 is generated while wave k is transported: its blocks
 // fill the SMs that wave k's finished warps leave. Counters are zeroed once
 // per batch. Returns the number of kernels launched.
-std::uint64_t LaunchBatchedWaves(g4b_handle& h, const LaunchParams& base, unsigned grid, std::uint32_t block) {
+void PrepareWaves(g4b_handle& h) {
     EnsureGenerationStream(h);
+    h.dStore.Ensure(2U * StoreBytes(WavePhotons(h)), "cudaMalloc photon stores");
+    h.dTickets.Ensure(2U * sizeof(unsigned int), "cudaMalloc work tickets");
+}
+
+std::uint64_t LaunchBatchedWaves(g4b_handle& h, const LaunchParams& base, unsigned grid, std::uint32_t block) {
+    PrepareWaves(h);
     const std::uint64_t wave{WavePhotons(h)};
     const std::uint64_t waves{(h.photonCount + wave - 1U) / wave};
-    h.dStore.Ensure(2U * StoreBytes(wave), "cudaMalloc photon stores");
-    h.dTickets.Ensure(2U * sizeof(unsigned int), "cudaMalloc work tickets");
     const auto waveParams{[&](std::uint64_t k) {
         LaunchParams p{base};
         p.photonBegin = static_cast<std::uint32_t>(k * wave);
@@ -807,6 +812,52 @@ std::uint64_t LaunchBatchedWaves(g4b_handle& h, const LaunchParams& base, unsign
     return launches;
 }
 
+// The generation-pass waves as a CUDA graph: captured from the two streams
+// on every run (the launch parameters and wave count follow the batch),
+// applied to the previous executable graph when its shape still fits and
+// instantiated afresh when it does not, then launched. Relaunches of a batch
+// therefore replay one graph of 2 + 3 x waves nodes.
+std::uint64_t LaunchBatchedWavesGraph(g4b_handle& h, const LaunchParams& base, unsigned grid, std::uint32_t block) {
+    PrepareWaves(h);  // allocations stay outside the capture
+    Check(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    cudaGraph_t graph{nullptr};
+    std::uint64_t launches{0};
+    try {
+        launches = LaunchBatchedWaves(h, base, grid, block);
+    } catch (...) {
+        cudaStreamEndCapture(h.stream, &graph);
+        if (graph != nullptr) {
+            cudaGraphDestroy(graph);
+        }
+        static_cast<void>(cudaGetLastError());
+        throw;
+    }
+    Check(cudaStreamEndCapture(h.stream, &graph), "cudaStreamEndCapture");
+    bool updated{false};
+    if (h.wavesExec != nullptr) {
+        cudaGraphExecUpdateResultInfo info{};
+        if (cudaGraphExecUpdate(h.wavesExec, graph, &info) == cudaSuccess) {
+            updated = true;
+        } else {
+            static_cast<void>(cudaGetLastError());  // a shape change is not an error: instantiate anew
+            cudaGraphExecDestroy(h.wavesExec);
+            h.wavesExec = nullptr;
+        }
+    }
+    if (!updated) {
+        const cudaError_t status{cudaGraphInstantiate(&h.wavesExec, graph, 0)};
+        if (status != cudaSuccess) {
+            h.wavesExec = nullptr;
+        }
+        cudaGraphDestroy(graph);
+        Check(status, "cudaGraphInstantiate");
+    } else {
+        cudaGraphDestroy(graph);
+    }
+    Check(cudaGraphLaunch(h.wavesExec, h.stream), "cudaGraphLaunch");
+    return launches;
+}
+
 // Hit rows reserved by default: a quarter of the photons (at least 2^20, at
 // most all of them). Overflow is caught after the launch and the batch is
 // rerun with an exact-size buffer, which gives identical results because
@@ -832,7 +883,8 @@ void RunStaged(g4b_handle& h) {
             base.chunk = RoundChunk(static_cast<std::uint32_t>(std::clamp<std::uint64_t>(perWarp, 32U, h.chunk)));
         }
         if (UsesGenerationPass(h)) {
-            h.launchCount += LaunchBatchedWaves(h, base, grid, h.blockSize);
+            h.launchCount += h.config.use_cuda_graph != 0 ? LaunchBatchedWavesGraph(h, base, grid, h.blockSize)
+                                                           : LaunchBatchedWaves(h, base, grid, h.blockSize);
         } else if (h.config.use_cuda_graph != 0) {
             LaunchBatchedGraph(h, base, grid);
             h.launchCount += 2;
@@ -1319,6 +1371,9 @@ int g4b_destroy(g4b_handle* handle) {
         cudaStreamSynchronize(handle->generationStream);
     }
     DestroyGraph(*handle);
+    if (handle->wavesExec != nullptr) {
+        cudaGraphExecDestroy(handle->wavesExec);
+    }
     handle->hostToDeviceTimer.Destroy();
     handle->memsetTimer.Destroy();
     handle->kernelTimer.Destroy();
