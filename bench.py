@@ -63,8 +63,8 @@ def scheduler_leg(scene, events: int, local: int, producers: int = 8, window: in
     (g4b_scheduler_replay), each keeping at most `window` results
     outstanding (the reference's maxPendingEvents per worker,
     PhotonTransportConfig.hpp:36): pipelined (two batches in flight) and in the reference's
-    serial order, both at the reference's batch target. Host wall clock from the first submission to the last result,
-    after one warm-up pass."""
+    serial order, both at the reference's batch target. Host wall clock from the first submission to the last result:
+    the better of two passes after one warm-up pass."""
     from g4go_b200 import PhotonTransportConfig, scenes
     from g4go_b200.scheduler import BatchSchedulerConfig, OpticalBatchScheduler, OpticalSubmission
 
@@ -80,16 +80,21 @@ def scheduler_leg(scene, events: int, local: int, producers: int = 8, window: in
                    for i, event_id in enumerate(batch.event_ids)]
     photons = int(sum(sub.photon_count for sub in submissions))
     out = {"unit": UNIT, "events": len(submissions), "photons": photons, "producers": producers,
-           "window": window, "timing": "host wall clock, first submission to last result, after a warm-up pass"}
+           "window": window, "timing": "host wall clock, first submission to last result; best of two passes after a warm-up pass"}
     runs = (("pipelined", BatchSchedulerConfig(enable_performance_diagnostics=True)),
             ("serial", BatchSchedulerConfig(serial=True, enable_performance_diagnostics=True)))
     for name, batching in runs:
         config = PhotonTransportConfig(seed=7, device=local)
         with OpticalBatchScheduler(config, scene, batching) as scheduler:
             scheduler.replay(submissions, producers, window)  # warm-up: engine handles, graphs, staging
-            before = scheduler.batch_statistics()
-            detections, seconds = scheduler.replay(submissions, producers, window)
-            after = scheduler.batch_statistics()
+            best = None
+            for _ in range(2):  # the better of two passes: host-side contention varies between passes
+                before = scheduler.batch_statistics()
+                detections, seconds = scheduler.replay(submissions, producers, window)
+                after = scheduler.batch_statistics()
+                if best is None or seconds < best[1]:
+                    best = (detections, seconds, before, after)
+            detections, seconds, before, after = best
         out[name] = {"value": photons / seconds, "seconds": seconds, "detections": detections,
                      "target_photons_per_batch": batching.target_photons_per_batch,
                      "batches": after["batch_count"] - before["batch_count"],

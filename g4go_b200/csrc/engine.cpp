@@ -221,10 +221,16 @@ namespace {
 int Precision(const g4b_handle& h) { return h.config.precision == G4B_PRECISION_FP64 ? g4b::kFP64 : g4b::kFP32; }
 int Form(const g4b_handle& h) { return h.config.launch_form == G4B_FORM_PLAIN ? g4b::kPlain : g4b::kBatched; }
 
-// The batched FP32 form makes its photons in a separate generation pass
-// unless the configuration asks for generation inside the transport loop.
+// The batched FP32 form makes the photons of a large batch in a separate
+// generation pass (config 0 or 1) unless the configuration asks for
+// generation inside the transport loop (2). A batch below
+// kGenerationPassMinPhotons keeps generation in the loop: a single wave has
+// nothing to overlap its generation with, and the transport of a small batch
+// is bound by its tail, so the pass only adds latency there.
+constexpr std::uint64_t kGenerationPassMinPhotons{1ULL << 24};
 bool UsesGenerationPass(const g4b_handle& h) {
-    return Form(h) == g4b::kBatched && Precision(h) == g4b::kFP32 && h.config.generation_pass != 2U;
+    return Form(h) == g4b::kBatched && Precision(h) == g4b::kFP32 && h.config.generation_pass != 2U &&
+           h.photonCount >= kGenerationPassMinPhotons;
 }
 
 // The kernel variant of a form: with the coincidence counters only when

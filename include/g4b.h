@@ -210,9 +210,11 @@ typedef struct g4b_config {
                                         picks one. Photons per thread per grab = chunk / 32. */
     uint32_t use_cuda_graph;         /* 1 -> batched launches replay a captured graph */
     uint32_t record_photon_fates;    /* 1 -> keep a per-photon fate/bounce/time record (diagnostics) */
-    uint32_t generation_pass;        /* batched FP32 form: 0 or 1 -> photons made by a separate generation
-                                        kernel into a photon store, in waves of up to 2^26 photons, and
-                                        read by the transport kernel; 2 -> made inside the transport loop */
+    uint32_t generation_pass;        /* batched FP32 form: 0 or 1 -> the photons of a batch of at least 2^24
+                                        photons are made by a separate generation kernel into a photon
+                                        store, in waves of up to 2^26 photons, and read by the transport
+                                        kernel (smaller batches generate inside the transport loop);
+                                        2 -> always inside the transport loop */
     uint32_t reserved[6];
 } g4b_config;
 
