@@ -400,6 +400,8 @@ def bench_ours(args, world, rank, local):
     peaks, peak_kind = measured_peaks()
     kernel_mean_ms = sum(kernel_ms) / len(kernel_ms)
     algorithmic_bytes = emissions * (128 + 4 + 4) + 4 + hits_per_step * 48 + events * 64 + 64
+    if photons >= 2 ** 24:  # the generation pass: each photon's 64-B store row written once and read once
+        algorithmic_bytes += photons * 128
     achieved_gbs = algorithmic_bytes / (kernel_mean_ms / 1000.0) / 1e9
     prof = profile_inputs()
     traffic = None
