@@ -8,9 +8,12 @@ the parity tests hold byte-exact against the oracle. Every photon comes from
 its own genstep and RNG counters either way, so the detections (in the
 reference's flattened-photon order) and every counter must be identical.
 """
+import ctypes as C
+
+import numpy as np
 import pytest
 
-from g4go_b200 import PhotonTransportConfig, TransportHost, scenes
+from g4go_b200 import DETECTION_DTYPE, PhotonTransportConfig, TransportHost, _abi, scenes
 
 pytestmark = pytest.mark.gpu
 
@@ -22,29 +25,63 @@ def large_batch():
     return scenes.crystal_sipm_scene(), batch
 
 
-def run(scene, batch, **config):
+def run(scene, batch, pinned=None, **config):
     with TransportHost(PhotonTransportConfig(seed=99, **config)) as host:
         host.enqueue_emissions(scene, batch)
-        out = host.complete_oldest_batch()
+        out = host.complete_oldest_batch(detections_out=pinned)
+        out.detections = out.detections.copy()
         host.relaunch()  # a replay of the same batch (the captured graph, updated in place)
-        again = host.complete_oldest_batch()
+        again = host.complete_oldest_batch(detections_out=pinned)
+        again.detections = again.detections.copy()
     return out, again
 
 
-@pytest.mark.parametrize("graph", [True, False])
-def test_generation_pass_matches_generation_in_the_loop(large_batch, graph):
+class PinnedDetections:
+    """A page-locked detection buffer (g4b_host_alloc): g4b_complete copies
+    the ordered detections straight into it."""
+
+    def __init__(self, rows):
+        self.lib = _abi.load()
+        self.pointer = C.c_void_p()
+        assert self.lib.g4b_host_alloc(rows * DETECTION_DTYPE.itemsize, C.byref(self.pointer)) == 0
+        raw = (C.c_ubyte * (rows * DETECTION_DTYPE.itemsize)).from_address(self.pointer.value)
+        self.array = np.frombuffer(raw, dtype=DETECTION_DTYPE)
+
+    def free(self):
+        self.array = None
+        self.lib.g4b_host_free(self.pointer)
+
+
+@pytest.mark.parametrize("graph,pinned,ordered", [(True, False, True), (False, False, True), (True, True, True),
+                                                  (False, True, True), (True, True, False)])
+def test_generation_pass_matches_generation_in_the_loop(large_batch, graph, pinned, ordered):
     scene, batch = large_batch
-    inline, _ = run(scene, batch, generation_pass=2, use_cuda_graph=graph)
-    passed, replayed = run(scene, batch, generation_pass=0, use_cuda_graph=graph)
+    buffer = PinnedDetections(batch.photon_count // 4) if pinned else None
+    try:
+        inline, _ = run(scene, batch, generation_pass=2, use_cuda_graph=graph, ordered_detections=ordered)
+        passed, replayed = run(scene, batch, pinned=buffer.array if pinned else None, generation_pass=0,
+                               use_cuda_graph=graph, ordered_detections=ordered)
+    finally:
+        if buffer is not None:
+            buffer.free()
     assert inline.statistics["detected_count"] > 0
     for out in (passed, replayed):
-        assert out.detections.tobytes() == inline.detections.tobytes()
+        assert same_detections(out.detections, inline.detections, ordered)
         assert counters(out.statistics) == counters(inline.statistics)
         assert [(e, counters(s)) for e, s in out.event_statistics] == \
             [(e, counters(s)) for e, s in inline.event_statistics]
         assert out.performance["total_bounce_count"] == inline.performance["total_bounce_count"]
     # two waves: zero, two generations, two transports
     assert passed.performance["kernel_launch_count"] >= 5
+
+
+def same_detections(a, b, ordered):
+    """Byte for byte; without the flattened-photon order, the rows come in the
+    order warps appended them, so they are compared sorted by event and photon."""
+    if not ordered:
+        a = a[np.lexsort((a["photon_id"], a["event_id"]))]
+        b = b[np.lexsort((b["photon_id"], b["event_id"]))]
+    return a.tobytes() == b.tobytes()
 
 
 def counters(statistics):
