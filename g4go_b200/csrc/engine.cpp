@@ -177,6 +177,16 @@ struct g4b_handle {
     cudaEvent_t generatedEvent[2]{};
     cudaEvent_t storeFreeEvent[2]{};
     cudaGraphExec_t wavesExec{nullptr};  // the generation-pass waves of the last batch, captured
+    // Per-wave ordering of the generation-pass form: after each wave's
+    // transport its hits are ordered into dDetections on the same stream, the
+    // hit-row counts before and after each wave kept in dWaveRows (copied to
+    // hWaveRows) and an event recorded, so g4b_complete can copy each wave's
+    // detections to the host while later waves run.
+    DeviceBuffer dWaveRows;
+    PinnedBuffer hWaveRows;
+    std::vector<cudaEvent_t> waveEvents;
+    std::uint64_t pendingWaves{0};  // waves of the pending batch ordered that way (0: none)
+    cudaStream_t copyStream{nullptr};
 
     // The staged batch (kept for g4b_relaunch) and the pending one.
     bool hasStaged{false};
@@ -712,7 +722,8 @@ void LaunchBatchedGraph(g4b_handle& h, const LaunchParams& params, unsigned grid
 // of at most kPhotonStoreWave.
 std::uint64_t WavePhotons(const g4b_handle& h) {
     const std::uint64_t waves{(h.photonCount + g4b::kPhotonStoreWave - 1U) / g4b::kPhotonStoreWave};
-    return waves == 0U ? 0U : (h.photonCount + waves - 1U) / waves;
+    // a multiple of 32, so every wave starts on a word of the slot bitmap
+    return waves == 0U ? 0U : ((h.photonCount + waves - 1U) / waves + 31U) / 32U * 32U;
 }
 
 // Bytes of one photon store for `rows` photons: 256-byte aligned columns.
@@ -771,11 +782,26 @@ void EnsureGenerationStream(g4b_handle& h) {
 // per batch. Returns the number of kernels launched.
 void PrepareWaves(g4b_handle& h) {
     EnsureGenerationStream(h);
-    h.dStore.Ensure(2U * StoreBytes(WavePhotons(h)), "cudaMalloc photon stores");
+    const std::uint64_t wave{WavePhotons(h)};
+    const std::uint64_t waves{(h.photonCount + wave - 1U) / wave};
+    h.dStore.Ensure(2U * StoreBytes(wave), "cudaMalloc photon stores");
     h.dTickets.Ensure(2U * sizeof(unsigned int), "cudaMalloc work tickets");
+    h.dWaveRows.Ensure((waves + 1U) * sizeof(unsigned long long), "cudaMalloc wave rows");
+    h.hWaveRows.Ensure((waves + 1U) * sizeof(unsigned long long), "cudaMallocHost wave rows");
+    while (h.waveEvents.size() < waves) {
+        cudaEvent_t event{nullptr};
+        Check(cudaEventCreateWithFlags(&event, cudaEventDisableTiming), "cudaEventCreate");
+        h.waveEvents.push_back(event);
+    }
+    const std::uint32_t words{static_cast<std::uint32_t>((h.photonCount + 31U) / 32U)};
+    h.dBitmap.Ensure(sizeof(std::uint32_t) * words, "cudaMalloc slot bitmap");
+    h.dPrefix.Ensure(sizeof(std::uint32_t) * words, "cudaMalloc slot prefix");
+    h.dBlockSums.Ensure(sizeof(std::uint32_t) * ((words + 1023U) / 1024U + 1U), "cudaMalloc block sums");
+    h.dDetections.Ensure(sizeof(g4b_photon_detection) * h.hitCapacity, "cudaMalloc detections");
 }
 
-std::uint64_t LaunchBatchedWaves(g4b_handle& h, const LaunchParams& base, unsigned grid, std::uint32_t block) {
+std::uint64_t LaunchBatchedWaves(g4b_handle& h, const LaunchParams& base, unsigned grid, std::uint32_t block,
+                                 bool capturing = false) {
     PrepareWaves(h);
     const std::uint64_t wave{WavePhotons(h)};
     const std::uint64_t waves{(h.photonCount + wave - 1U) / wave};
@@ -789,6 +815,8 @@ std::uint64_t LaunchBatchedWaves(g4b_handle& h, const LaunchParams& base, unsign
     }};
     const unsigned generateGrid{static_cast<unsigned>(h.smCount) * 8U};
     Check(g4b::LaunchZeroCounters(base.events, base.eventCount, base.run, h.stream), "zero counters");
+    auto* waveRows{h.dWaveRows.As<unsigned long long>()};
+    Check(cudaMemsetAsync(waveRows, 0, sizeof(unsigned long long), h.stream), "zero wave rows");
     Check(cudaEventRecord(h.zeroedEvent, h.stream), "cudaEventRecord");
     Check(cudaStreamWaitEvent(h.generationStream, h.zeroedEvent, 0), "cudaStreamWaitEvent");
     Check(g4b::LaunchGenerate(waveParams(0), generateGrid, SceneSharedBytes(h), h.generationStream),
@@ -804,6 +832,24 @@ std::uint64_t LaunchBatchedWaves(g4b_handle& h, const LaunchParams& base, unsign
               "transport launch");
         Check(cudaEventRecord(h.storeFreeEvent[k % 2U], h.stream), "cudaEventRecord");
         ++launches;
+        // order this wave's hits while the next wave is generated
+        Check(cudaMemcpyAsync(waveRows + k + 1U, &base.run->hitCount, sizeof(unsigned long long),
+                              cudaMemcpyDeviceToDevice, h.stream),
+              "cudaMemcpyAsync wave rows");
+        const bool ordered{h.config.ordered_detections != 0};
+        Check(g4b::LaunchOrderWaveHits(base.hits, waveRows + k, p.photonBegin, p.photonEnd, h.dBitmap.As<std::uint32_t>(),
+                                       h.dPrefix.As<std::uint32_t>(), h.dBlockSums.As<std::uint32_t>(),
+                                       h.dDetections.pointer, ordered, static_cast<unsigned>(h.smCount) * 4U,
+                                       h.stream),
+              "wave hit ordering");
+        launches += ordered ? 5U : 1U;
+        Check(cudaMemcpyAsync(h.hWaveRows.As<unsigned long long>() + k + 1U, waveRows + k + 1U,
+                              sizeof(unsigned long long), cudaMemcpyDeviceToHost, h.stream),
+              "cudaMemcpyAsync wave rows to host");
+        // inside a capture the record must stay a real event record for the host to wait on
+        Check(capturing ? cudaEventRecordWithFlags(h.waveEvents[k], h.stream, cudaEventRecordExternal)
+                        : cudaEventRecord(h.waveEvents[k], h.stream),
+              "cudaEventRecord wave");
         if (k + 1U < waves) {
             if (k >= 1U) {  // the next wave's store and ticket were last used by wave k - 1
                 Check(cudaStreamWaitEvent(h.generationStream, h.storeFreeEvent[(k + 1U) % 2U], 0),
@@ -829,7 +875,7 @@ std::uint64_t LaunchBatchedWavesGraph(g4b_handle& h, const LaunchParams& base, u
     cudaGraph_t graph{nullptr};
     std::uint64_t launches{0};
     try {
-        launches = LaunchBatchedWaves(h, base, grid, block);
+        launches = LaunchBatchedWaves(h, base, grid, block, true);
     } catch (...) {
         cudaStreamEndCapture(h.stream, &graph);
         if (graph != nullptr) {
@@ -888,9 +934,11 @@ void RunStaged(g4b_handle& h) {
             const std::uint64_t perWarp{photons / (warps * 8U)};
             base.chunk = RoundChunk(static_cast<std::uint32_t>(std::clamp<std::uint64_t>(perWarp, 32U, h.chunk)));
         }
+        h.pendingWaves = 0;
         if (UsesGenerationPass(h)) {
             h.launchCount += h.config.use_cuda_graph != 0 ? LaunchBatchedWavesGraph(h, base, grid, h.blockSize)
                                                            : LaunchBatchedWaves(h, base, grid, h.blockSize);
+            h.pendingWaves = (h.photonCount + WavePhotons(h) - 1U) / WavePhotons(h);
         } else if (h.config.use_cuda_graph != 0) {
             LaunchBatchedGraph(h, base, grid);
             h.launchCount += 2;
@@ -968,6 +1016,7 @@ void Stage(g4b_handle& h, const g4b_optical_emission* emissions, std::uint32_t e
     }
 
     h.hasStaged = false;
+    h.pendingWaves = 0;
     h.emissionCount = emissionCount;
     h.eventCount = eventCount;
     h.photonCount = photonCount;
@@ -1154,10 +1203,64 @@ void FillStatistics(const g4b_handle& h, g4b_output& output) {
     output.statistics = batch;
 }
 
+// Detections of a batch already ordered wave by wave during its transport
+// (the generation-pass form): each wave's records are copied to a pinned
+// caller buffer as soon as that wave has finished, on the copy stream, while
+// the later waves still run; a pageable buffer gets them in one copy at the
+// end. Returns false when they cannot come from there (the device hit buffer
+// overflowed and the batch will rerun, or the caller's buffer is too small):
+// the whole-batch path then takes over.
+bool CompleteByWaves(g4b_handle& h, g4b_output& output) {
+    if (h.pendingWaves == 0U || output.detections == nullptr || output.detection_capacity == 0U) {
+        return false;
+    }
+    cudaPointerAttributes attributes{};
+    const bool pinned{cudaPointerGetAttributes(&attributes, output.detections) == cudaSuccess &&
+                      attributes.type == cudaMemoryTypeHost};
+    static_cast<void>(cudaGetLastError());
+    if (h.copyStream == nullptr) {
+        Check(cudaStreamCreateWithFlags(&h.copyStream, cudaStreamNonBlocking), "cudaStreamCreateWithFlags");
+    }
+    const auto* records{static_cast<const g4b_photon_detection*>(h.dDetections.pointer)};
+    auto* target{static_cast<g4b_photon_detection*>(output.detections)};
+    const auto* rows{h.hWaveRows.As<unsigned long long>()};
+    std::uint64_t copied{0};
+    Check(cudaEventRecord(h.hitsTimer.start, h.copyStream), "cudaEventRecord");
+    for (std::uint64_t k{0}; k < h.pendingWaves; ++k) {
+        Check(cudaEventSynchronize(h.waveEvents[k]), "cudaEventSynchronize wave");
+        const std::uint64_t end{rows[k + 1U]};
+        if (end > h.hitCapacity || end > output.detection_capacity) {
+            Check(cudaStreamSynchronize(h.copyStream), "cudaStreamSynchronize");
+            return false;
+        }
+        if (pinned && end > copied) {
+            Check(cudaMemcpyAsync(target + copied, records + copied, sizeof(g4b_photon_detection) * (end - copied),
+                                  cudaMemcpyDeviceToHost, h.copyStream),
+                  "cudaMemcpyAsync detections");
+            copied = end;
+        }
+    }
+    if (!pinned) {
+        copied = rows[h.pendingWaves];
+        const std::size_t bytes{sizeof(g4b_photon_detection) * copied};
+        h.hDetections.Ensure(bytes, "cudaMallocHost detections");
+        Check(cudaMemcpyAsync(h.hDetections.pointer, records, bytes, cudaMemcpyDeviceToHost, h.copyStream),
+              "cudaMemcpyAsync detections");
+        Check(cudaStreamSynchronize(h.copyStream), "cudaStreamSynchronize");
+        std::memcpy(target, h.hDetections.pointer, bytes);
+    }
+    Check(cudaEventRecord(h.hitsTimer.stop, h.copyStream), "cudaEventRecord");
+    Check(cudaStreamSynchronize(h.copyStream), "cudaStreamSynchronize");
+    WaitMetadata(h);  // every wave has finished without overflow: no rerun happens here
+    return h.hRun.As<RunCounters>()->hitCount == copied;
+}
+
 void Complete(g4b_handle& h, g4b_output& output) {
     if (!h.busy) {
         Throw(G4B_ERR_LOGIC, "transport queue is empty");
     }
+    const auto wavesStart{std::chrono::steady_clock::now()};
+    const bool byWaves{CompleteByWaves(h, output)};
     WaitMetadata(h);
     const bool transported{h.emissionCount != 0 && h.photonCount != 0};
     const std::uint64_t hits{transported ? h.hRun.As<RunCounters>()->hitCount : 0};
@@ -1171,7 +1274,12 @@ void Complete(g4b_handle& h, g4b_output& output) {
         Throw(G4B_ERR_CAPACITY, "output buffers are too small for the pending batch");
     }
     output.performance = g4b_performance{};
-    if (hits != 0 && !countsOnly) {
+    if (byWaves) {
+        output.performance.device_hits_to_host_ms = h.hitsTimer.Milliseconds();
+        output.performance.device_hits_to_host_bytes = sizeof(g4b_photon_detection) * hits;
+        output.performance.host_hit_compaction_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wavesStart).count();
+    } else if (hits != 0 && !countsOnly) {
         const std::uint32_t words{static_cast<std::uint32_t>((h.photonCount + 31U) / 32U)};
         const bool ordered{h.config.ordered_detections != 0};
         if (ordered) {
@@ -1393,6 +1501,13 @@ int g4b_destroy(g4b_handle* handle) {
         if (event != nullptr) {
             cudaEventDestroy(event);
         }
+    }
+    for (cudaEvent_t event : handle->waveEvents) {
+        cudaEventDestroy(event);
+    }
+    if (handle->copyStream != nullptr) {
+        cudaStreamSynchronize(handle->copyStream);
+        cudaStreamDestroy(handle->copyStream);
     }
     if (handle->generationStream != nullptr) {
         cudaStreamDestroy(handle->generationStream);

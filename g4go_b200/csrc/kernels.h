@@ -46,6 +46,16 @@ cudaError_t LaunchOrderHits(const HitColumns& hits, unsigned long long count, st
                             std::uint32_t* bitmap, std::uint32_t* prefix, std::uint32_t* blockSums,
                             void* detectionsOut, bool ordered, cudaStream_t stream);
 
+// Ordering of one wave's hits on the transport's stream: its hit rows are
+// [rows[0], rows[1]) (device memory, clamped to hits.capacity), its slots lie
+// in [slotBegin, slotEnd) (slotBegin a multiple of 32), and its records are
+// written to the same rows of detectionsOut, in slot order within the wave.
+// Five launches when ordered (after a bitmap-range clear), one otherwise.
+cudaError_t LaunchOrderWaveHits(const HitColumns& hits, const unsigned long long* rows, std::uint32_t slotBegin,
+                                std::uint32_t slotEnd, std::uint32_t* bitmap, std::uint32_t* prefix,
+                                std::uint32_t* blockSums, void* detectionsOut, bool ordered, unsigned grid,
+                                cudaStream_t stream);
+
 // Ordering of caller-owned detection records by a unique slot key below
 // slotLimit (at most kStaticOrderMaxSlots) with all scratch in one array
 // compiled into the library. StaticOrderScratch gives that array's address on

@@ -1043,6 +1043,44 @@ static __device__ __align__(256) std::uint32_t gStaticOrderScratch[kStaticScratc
 
 // Marks each record's slot key in the bitmap. A key at or above slotLimit,
 // or one already marked, touches nothing and adds one to *status.
+// Per-wave ordering on the transport's stream: the wave's hit rows are
+// [rows[0], rows[1]) of the hit buffer (device-side counts, clamped to the
+// buffer's capacity), their slots lie in the wave's slot range, and the
+// records go to the same rows of the detection buffer, ranked within the wave.
+__global__ void MarkWaveSlots(const std::uint32_t* __restrict__ slots, const unsigned long long* __restrict__ rows,
+                              unsigned long long capacity, std::uint32_t* __restrict__ bitmap) {
+    const unsigned long long begin{min(rows[0], capacity)};
+    const unsigned long long end{min(rows[1], capacity)};
+    for (unsigned long long i = begin + blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x;
+         i < end; i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+        const std::uint32_t slot{slots[i]};
+        atomicOr(bitmap + (slot >> 5U), 1U << (slot & 31U));
+    }
+}
+
+__global__ void ScatterWaveDetections(const HitColumns hits, const unsigned long long* __restrict__ rows,
+                                      unsigned long long capacity, const std::uint32_t* __restrict__ bitmap,
+                                      const std::uint32_t* __restrict__ prefix, bool ordered,
+                                      float4* __restrict__ out) {
+    const unsigned long long begin{min(rows[0], capacity)};
+    const unsigned long long end{min(rows[1], capacity)};
+    for (unsigned long long i = begin + blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x;
+         i < end; i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+        unsigned long long row{i};
+        if (ordered) {
+            const std::uint32_t slot{hits.slot[i]};
+            const std::uint32_t word{slot >> 5U};
+            const std::uint32_t below{bitmap[word] & ((1U << (slot & 31U)) - 1U)};
+            row = begin + prefix[word] + static_cast<std::uint32_t>(__popc(below));
+        }
+        float4* record{out + row * 3ULL};
+        record[0] = make_float4(hits.positionX[i], hits.positionY[i], hits.positionZ[i], hits.time[i]);
+        record[1] = make_float4(hits.directionX[i], hits.directionY[i], hits.directionZ[i], hits.energy[i]);
+        record[2] = make_float4(__uint_as_float(hits.eventID[i]), __uint_as_float(hits.photonID[i]),
+                                __uint_as_float(hits.sensorID[i]), 0.0F);
+    }
+}
+
 __global__ void MarkKeysChecked(const std::uint32_t* __restrict__ keys, unsigned long long count,
                                 std::uint32_t slotLimit, std::uint32_t* __restrict__ bitmap,
                                 std::uint32_t* __restrict__ status) {
@@ -1243,6 +1281,28 @@ cudaError_t LaunchOrderHits(const HitColumns& hits, unsigned long long count, st
     }
     ScatterDetections<<<BlocksFor(count, 256U), 256, 0, stream>>>(hits, count, bitmap, prefix, ordered,
                                                                   static_cast<float4*>(detectionsOut));
+    return cudaGetLastError();
+}
+
+cudaError_t LaunchOrderWaveHits(const HitColumns& hits, const unsigned long long* rows, std::uint32_t slotBegin,
+                                std::uint32_t slotEnd, std::uint32_t* bitmap, std::uint32_t* prefix,
+                                std::uint32_t* blockSums, void* detectionsOut, bool ordered, unsigned grid,
+                                cudaStream_t stream) {
+    if (ordered) {
+        const std::uint32_t wordBegin{slotBegin / 32U};
+        const std::uint32_t words{(slotEnd - slotBegin + 31U) / 32U};
+        const std::uint32_t blocks{(words + 1023U) / 1024U};
+        cudaError_t error{cudaMemsetAsync(bitmap + wordBegin, 0, static_cast<std::size_t>(words) * 4U, stream)};
+        if (error != cudaSuccess) {
+            return error;
+        }
+        MarkWaveSlots<<<grid, 256, 0, stream>>>(hits.slot, rows, hits.capacity, bitmap);
+        BlockPopcount<<<blocks, 256, 0, stream>>>(bitmap + wordBegin, words, blockSums);
+        ScanBlockSums<<<1, 1024, 0, stream>>>(blockSums, blocks);
+        WordPrefix<<<blocks, 256, 0, stream>>>(bitmap + wordBegin, words, blockSums, prefix + wordBegin);
+    }
+    ScatterWaveDetections<<<grid, 256, 0, stream>>>(hits, rows, hits.capacity, bitmap, prefix, ordered,
+                                                    static_cast<float4*>(detectionsOut));
     return cudaGetLastError();
 }
 

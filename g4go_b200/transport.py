@@ -411,6 +411,14 @@ class TransportHost:
 
         counts_only: return statistics without copying the detections back
         (they stay in device memory)."""
+        if detections_out is not None and not counts_only and self._pending_batch is not None:
+            # a caller buffer: complete at once, without first waiting for the
+            # counts, so that a multi-wave batch's detections stream into it
+            # while its later waves still run; too small -> the counts first
+            events = int(self._pending_batch.event_ids.shape[0])
+            done = self._complete_into(detections_out, detections_out.shape[0], events)
+            if done is not None:
+                return done
         count, events = self.query_oldest()
         if counts_only:
             detections_out = np.empty(0, dtype=DETECTION_DTYPE)
@@ -428,6 +436,29 @@ class TransportHost:
         event_list = [(int(event_stats[i].event_id), _stats_dict(event_stats[i].statistics)) for i in range(events)]
         return PhotonTransportOutput(
             detections=detections_out[: 0 if counts_only else output.detection_count],
+            statistics=_stats_dict(output.statistics),
+            performance=perf,
+            event_statistics=event_list,
+        )
+
+    def _complete_into(self, detections_out: np.ndarray, capacity: int, events: int):
+        """g4b_complete into the caller's buffer; None if it is too small (the batch stays pending)."""
+        event_stats = (_abi.EventStatistics * max(events, 1))()
+        output = _abi.Output()
+        output.detections = detections_out.ctypes.data_as(C.c_void_p)
+        output.detection_capacity = capacity
+        output.event_statistics = C.cast(event_stats, C.POINTER(_abi.EventStatistics))
+        output.event_capacity = events
+        status = self._lib.g4b_complete(self._handle, C.byref(output))
+        if status == _abi.ERR_CAPACITY:
+            return None
+        self._check(status)
+        self._pending_batch = None
+        perf = {name: getattr(output.performance, name) for name in PERF_FIELDS}
+        event_list = [(int(event_stats[i].event_id), _stats_dict(event_stats[i].statistics))
+                      for i in range(output.event_count)]
+        return PhotonTransportOutput(
+            detections=detections_out[: output.detection_count],
             statistics=_stats_dict(output.statistics),
             performance=perf,
             event_statistics=event_list,
