@@ -263,7 +263,8 @@ std::size_t SharedBytes(const g4b_handle& h, int form, std::uint32_t blockSize) 
     if (form == g4b::kBatched) {
         const bool fp64{h.config.precision == G4B_PRECISION_FP64};
         const std::size_t queue{UsesGenerationPass(h) ? 0U : (fp64 ? g4b::kQueueBytesFP64 : g4b::kQueueBytesFP32)};
-        const std::size_t ring{fp64 ? g4b::kRingBytesFP64 : g4b::kRingBytesFP32};
+        const std::size_t ring{fp64 ? g4b::kRingBytesFP64
+                                    : (UsesGenerationPass(h) ? g4b::kRingBytesFP32Pass : g4b::kRingBytesFP32)};
         bytes += (queue + ring) * (blockSize / 32U) + g4b::kLaneTallyBytes * blockSize;
     }
     return bytes;

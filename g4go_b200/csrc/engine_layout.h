@@ -106,6 +106,12 @@ constexpr std::uint32_t kQueueBytesFP64 = 10U * 32U * 8U + 32U * 8U + 5U * 32U *
 constexpr std::uint32_t kFresnelRingEntries = 40;
 constexpr std::uint32_t kRingBytesFP32 = kFresnelRingEntries * (12U * 4U + 8U + 7U * 4U);  // 3360
 constexpr std::uint32_t kRingBytesFP64 = kFresnelRingEntries * (12U * 8U + 8U + 7U * 4U);  // 5280
+// The ring of the form with a generation pass (no photon queue in shared
+// memory): 64 entries, more than one step can ever need (at most 31 ready or
+// pending entries between steps, plus 32 parking), so that form has no
+// full-ring fallback; three blocks use 191 KB of shared memory per SM.
+constexpr std::uint32_t kFresnelRingEntriesPass = 64;
+constexpr std::uint32_t kRingBytesFP32Pass = kFresnelRingEntriesPass * (12U * 4U + 8U + 7U * 4U);  // 5376
 // Per-thread event counters and bounce total of the batched form, kept in
 // shared memory instead of registers (they change once per photon).
 constexpr std::uint32_t kLaneTallyBytes = 40;

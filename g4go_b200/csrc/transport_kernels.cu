@@ -313,9 +313,9 @@ static_assert(sizeof(WarpQueue<double>) == kQueueBytesFP64, "queue layout");
 // warp completes them together (one job per lane) and they stay in place as
 // ready photons, which idle lanes take before fresh ones. Entries are used in
 // ring order: [readyHead, pendingHead) ready, [pendingHead, pendingEnd) pending.
-template<class R>
+template<class R, std::uint32_t kRingEntries = kFresnelRingEntries>
 struct FresnelRing {
-    static constexpr std::uint32_t kEntries = kFresnelRingEntries;
+    static constexpr std::uint32_t kEntries = kRingEntries;
     R positionX[kEntries], positionY[kEntries], positionZ[kEntries];  // the boundary point while pending
     R directionX[kEntries], directionY[kEntries], directionZ[kEntries];
     R polarizationX[kEntries], polarizationY[kEntries], polarizationZ[kEntries];
@@ -392,6 +392,7 @@ struct FresnelRing {
 };
 static_assert(sizeof(FresnelRing<float>) == kRingBytesFP32, "ring layout");
 static_assert(sizeof(FresnelRing<double>) == kRingBytesFP64, "ring layout");
+static_assert(sizeof(FresnelRing<float, kFresnelRingEntriesPass>) == kRingBytesFP32Pass, "ring layout");
 
 
 // A Fresnel step completed in the lane that reached it, when the ring is full.
@@ -404,11 +405,11 @@ G4B_COLD std::uint32_t FinishFresnelHere(Photon<R>& photon, const FresnelJob<R>&
 
 // Completes `count` (<= 32) pending Fresnel jobs from pendingHead, one per
 // lane, leaving them in place as ready photons.
-template<class R>
-__device__ __forceinline__ void ResolvePending(FresnelRing<R>& ring, std::uint32_t& pendingHead, std::uint32_t count,
+template<class R, class Ring>
+__device__ __forceinline__ void ResolvePending(Ring& ring, std::uint32_t& pendingHead, std::uint32_t count,
                                                unsigned lane, const LaunchParams& p, R epsilon) {
     if (lane < count) {
-        const unsigned k{(pendingHead + lane) % FresnelRing<R>::kEntries};
+        const unsigned k{(pendingHead + lane) % Ring::kEntries};
         Photon<R> photon{};
         FresnelJob<R> job;
         ring.TakeJob(k, photon, job);
@@ -459,11 +460,11 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
     const std::uint32_t warps{blockDim.x >> 5U};
     constexpr std::uint32_t kQueueBytes{kPregenerated ? 0U : static_cast<std::uint32_t>(sizeof(WarpQueue<R>))};
     WarpQueue<R>& queue{*reinterpret_cast<WarpQueue<R>*>(gShared + sceneEnd + (threadIdx.x >> 5U) * kQueueBytes)};
-    FresnelRing<R>& ring{*reinterpret_cast<FresnelRing<R>*>(gShared + sceneEnd + warps * kQueueBytes +
-                                                            (threadIdx.x >> 5U) * sizeof(FresnelRing<R>))};
-    LaneTally& tally{*reinterpret_cast<LaneTally*>(gShared + sceneEnd + warps * (kQueueBytes + sizeof(FresnelRing<R>)) +
+    using Ring = FresnelRing<R, kPregenerated ? kFresnelRingEntriesPass : kFresnelRingEntries>;
+    Ring& ring{*reinterpret_cast<Ring*>(gShared + sceneEnd + warps * kQueueBytes + (threadIdx.x >> 5U) * sizeof(Ring))};
+    LaneTally& tally{*reinterpret_cast<LaneTally*>(gShared + sceneEnd + warps * (kQueueBytes + sizeof(Ring)) +
                                                    threadIdx.x * sizeof(LaneTally))};
-    constexpr std::uint32_t kRing{FresnelRing<R>::kEntries};
+    constexpr std::uint32_t kRing{Ring::kEntries};
     std::uint32_t readyHead{0U};
     std::uint32_t pendingHead{0U};
     std::uint32_t pendingEnd{0U};
@@ -637,7 +638,20 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
         }
         const bool parking{alive && result == kFresnelPending};
         const unsigned parkMask{__ballot_sync(kFullMask, parking)};
-        if (parkMask != 0U) {
+        if constexpr (kRing >= 2U * 32U - 1U) {
+            // The ring cannot be full. Between steps at most 31 entries are
+            // ready or pending: pending ones stay below 32 (32 are completed
+            // whenever 32 wait), and the lanes that parked in one step take
+            // ready entries first in the next, as many as they are, which is
+            // at least as many as a completion of 32 added beyond the 32
+            // that parked. So up to 32 parking photons always fit, and the
+            // live photon never has its address taken by a fallback.
+            if (parking) {
+                ring.PutJob((pendingEnd + static_cast<std::uint32_t>(__popc(parkMask & lanesBelow))) % kRing, photon,
+                            job);
+            }
+            pendingEnd += static_cast<std::uint32_t>(__popc(parkMask));
+        } else if (parkMask != 0U) {
             const std::uint32_t room{kRing - (pendingEnd - readyHead)};
             if (parking) {
                 const std::uint32_t rank{static_cast<std::uint32_t>(__popc(parkMask & lanesBelow))};
