@@ -18,6 +18,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <utility>
 #include <vector>
@@ -980,6 +981,46 @@ void RunStaged(g4b_handle& h) {
     h.fatesValid = h.config.record_photon_fates != 0;
 }
 
+// Host threads for the staging loops of a batch: reading and copying the
+// gensteps is memory bound on one thread (241 MB for 1.9e6 gensteps). At least
+// 2^16 gensteps per thread, at most 16 threads, and, where each thread keeps
+// its own per-event tallies, at most 2^24 tally entries in all.
+unsigned StagingThreads(std::uint64_t items, std::uint64_t tallyEntries = 0) {
+    std::uint64_t threads{std::min<std::uint64_t>(std::max(1U, std::thread::hardware_concurrency()), 16U)};
+    threads = std::min(threads, std::max<std::uint64_t>(items >> 16U, 1U));
+    if (tallyEntries != 0) {
+        threads = std::min(threads, std::max<std::uint64_t>((1ULL << 24U) / tallyEntries, 1U));
+    }
+    return static_cast<unsigned>(threads);
+}
+
+// body(begin, end, t) over `threads` contiguous parts of [0, count); part 0 on
+// the calling thread. The body must not throw. A thread that cannot be started
+// leaves its part to the calling thread.
+template<class Body>
+void ParallelRanges(std::uint32_t count, unsigned threads, const Body& body) {
+    const auto begin{[&](unsigned t) {
+        return static_cast<std::uint32_t>(static_cast<std::uint64_t>(count) * t / threads);
+    }};
+    std::vector<std::thread> pool;
+    unsigned started{1U};
+    try {
+        pool.reserve(threads - 1U);
+        for (; started < threads; ++started) {
+            pool.emplace_back(body, begin(started), begin(started + 1U), started);
+        }
+    } catch (...) {
+        // fewer threads than asked for: the remaining parts run below
+    }
+    for (unsigned t{started}; t < threads; ++t) {
+        body(begin(t), begin(t + 1U), t);
+    }
+    body(begin(0U), begin(1U), 0U);
+    for (auto& thread : pool) {
+        thread.join();
+    }
+}
+
 void Stage(g4b_handle& h, const g4b_optical_emission* emissions, std::uint32_t emissionCount,
            const std::uint32_t* eventIDs, std::uint32_t eventCount, const std::uint32_t* emissionEventIndices) {
     if (!h.hasScene) {
@@ -1000,17 +1041,43 @@ void Stage(g4b_handle& h, const g4b_optical_emission* emissions, std::uint32_t e
             Throw(G4B_ERR_INVALID_ARGUMENT, "event batch contains duplicate event IDs");
         }
     }
-    std::vector<std::uint64_t> captured(eventCount, 0);
-    std::vector<std::uint8_t> hasEmission(eventCount, 0);
-    std::uint64_t photonCount{0};
-    for (std::uint32_t i{}; i < emissionCount; ++i) {
-        const auto index{emissionEventIndices[i]};
-        if (index >= eventCount || emissions[i].event_id != eventIDs[index]) {
-            Throw(G4B_ERR_INVALID_ARGUMENT, "emission event index does not match event ID");
+    // per-event photon totals, in parallel parts with their own tallies; the
+    // first mismatching emission of any part fails the batch
+    const unsigned tallyThreads{StagingThreads(emissionCount, eventCount)};
+    std::vector<std::vector<std::uint64_t>> capturedBy(tallyThreads);
+    std::vector<std::vector<std::uint8_t>> hasEmissionBy(tallyThreads);
+    std::vector<std::uint64_t> photonsBy(tallyThreads, 0);
+    std::vector<std::uint8_t> mismatchBy(tallyThreads, 0);
+    ParallelRanges(emissionCount, tallyThreads, [&](std::uint32_t begin, std::uint32_t end, unsigned t) {
+        std::vector<std::uint64_t>& captured{capturedBy[t]};
+        std::vector<std::uint8_t>& hasEmission{hasEmissionBy[t]};
+        captured.assign(eventCount, 0);
+        hasEmission.assign(eventCount, 0);
+        std::uint64_t photons{0};
+        for (std::uint32_t i{begin}; i < end; ++i) {
+            const auto index{emissionEventIndices[i]};
+            if (index >= eventCount || emissions[i].event_id != eventIDs[index]) {
+                mismatchBy[t] = 1;
+                return;
+            }
+            captured[index] += emissions[i].photon_count;
+            hasEmission[index] = 1;
+            photons += emissions[i].photon_count;
         }
-        captured[index] += emissions[i].photon_count;
-        hasEmission[index] = 1;
-        photonCount += emissions[i].photon_count;
+        photonsBy[t] = photons;
+    });
+    if (std::find(mismatchBy.begin(), mismatchBy.end(), 1) != mismatchBy.end()) {
+        Throw(G4B_ERR_INVALID_ARGUMENT, "emission event index does not match event ID");
+    }
+    std::vector<std::uint64_t> captured{std::move(capturedBy[0])};
+    std::vector<std::uint8_t> hasEmission{std::move(hasEmissionBy[0])};
+    std::uint64_t photonCount{photonsBy[0]};
+    for (unsigned t{1U}; t < tallyThreads; ++t) {
+        for (std::uint32_t e{}; e < eventCount; ++e) {
+            captured[e] += capturedBy[t][e];
+            hasEmission[e] |= hasEmissionBy[t][e];
+        }
+        photonCount += photonsBy[t];
     }
     if (photonCount > 0xffffffffULL) {
         Throw(G4B_ERR_OVERFLOW, "emission batch exceeds the supported photon count");
@@ -1035,11 +1102,12 @@ void Stage(g4b_handle& h, const g4b_optical_emission* emissions, std::uint32_t e
     // Launch order: the batch order for the batched form; for the plain form
     // each event's emissions must be contiguous, so they are grouped by event
     // (stable) and every emission keeps its original flattened slot.
-    std::vector<std::uint32_t> order(emissionCount);
-    for (std::uint32_t i{}; i < emissionCount; ++i) {
-        order[i] = i;
-    }
+    std::vector<std::uint32_t> order;
     if (Form(h) == g4b::kPlain) {
+        order.resize(emissionCount);
+        for (std::uint32_t i{}; i < emissionCount; ++i) {
+            order[i] = i;
+        }
         std::stable_sort(order.begin(), order.end(), [&](std::uint32_t a, std::uint32_t b) {
             return emissionEventIndices[a] < emissionEventIndices[b];
         });
@@ -1068,26 +1136,69 @@ void Stage(g4b_handle& h, const g4b_optical_emission* emissions, std::uint32_t e
     auto* stagedEmissions{h.hEmissions.As<g4b_optical_emission>()};
     auto* offsets{h.hOffsets.As<std::uint32_t>()};
     auto* indices{h.hEventIndices.As<std::uint32_t>()};
+    auto* slotBase{h.usesSlotBase ? h.hSlotBase.As<std::uint32_t>() : nullptr};
+    const std::uint32_t* launchOrder{order.empty() ? nullptr : order.data()};
+    // Staged in parallel parts of the launch order: each part copies its
+    // records into pinned memory, maps their volume IDs (keeping the last
+    // lookup: consecutive gensteps mostly share a volume) and writes offsets
+    // relative to its first emission; the parts' totals are added after.
+    constexpr std::uint32_t kNoFailure{0xffffffffU};
+    const unsigned stageThreads{StagingThreads(emissionCount)};
+    std::vector<std::uint32_t> partPhotons(stageThreads, 0);
+    std::vector<std::uint32_t> failedAt(stageThreads, kNoFailure);
+    std::vector<std::uint8_t> unknownVolume(stageThreads, 0);
+    ParallelRanges(emissionCount, stageThreads, [&](std::uint32_t begin, std::uint32_t end, unsigned t) {
+        bool cached{false};
+        std::uint32_t lastVolumeID{0};
+        std::uint32_t lastVolume{0};
+        std::uint32_t running{0};
+        for (std::uint32_t k{begin}; k < end; ++k) {
+            const std::uint32_t i{launchOrder != nullptr ? launchOrder[k] : k};
+            g4b_optical_emission record{emissions[i]};
+            if (!cached || record.volume_id != lastVolumeID) {
+                const auto volume{h.volumeIndex.find(record.volume_id)};
+                if (volume == h.volumeIndex.end()) {
+                    failedAt[t] = k;
+                    unknownVolume[t] = 1;
+                    return;
+                }
+                cached = true;
+                lastVolumeID = record.volume_id;
+                lastVolume = volume->second;
+            }
+            if (record.material_id >= h.materialCount) {
+                failedAt[t] = k;
+                return;
+            }
+            record.volume_id = lastVolume;
+            stagedEmissions[k] = record;
+            indices[k] = emissionEventIndices[i];
+            if (slotBase != nullptr) {
+                slotBase[k] = originalOffsets[i];
+            }
+            running += record.photon_count;
+            offsets[k + 1] = running;
+        }
+        partPhotons[t] = running;
+    });
+    // the first failing emission in launch order, as a sequential pass finds it
+    for (unsigned t{}; t < stageThreads; ++t) {
+        if (failedAt[t] != kNoFailure) {
+            Throw(G4B_ERR_INVALID_ARGUMENT, unknownVolume[t] != 0 ? "emission references an unknown scene volume ID"
+                                                                  : "emission references an unknown scene material ID");
+        }
+    }
     offsets[0] = 0;
-    std::uint32_t running{0};
-    for (std::uint32_t k{}; k < emissionCount; ++k) {
-        const auto i{order[k]};
-        g4b_optical_emission record{emissions[i]};
-        const auto volume{h.volumeIndex.find(record.volume_id)};
-        if (volume == h.volumeIndex.end()) {
-            Throw(G4B_ERR_INVALID_ARGUMENT, "emission references an unknown scene volume ID");
+    if (stageThreads > 1U) {
+        std::vector<std::uint32_t> partBase(stageThreads, 0);
+        for (unsigned t{1U}; t < stageThreads; ++t) {
+            partBase[t] = partBase[t - 1U] + partPhotons[t - 1U];
         }
-        if (record.material_id >= h.materialCount) {
-            Throw(G4B_ERR_INVALID_ARGUMENT, "emission references an unknown scene material ID");
-        }
-        record.volume_id = volume->second;
-        stagedEmissions[k] = record;
-        indices[k] = emissionEventIndices[i];
-        if (h.usesSlotBase) {
-            h.hSlotBase.As<std::uint32_t>()[k] = originalOffsets[i];
-        }
-        running += record.photon_count;
-        offsets[k + 1] = running;
+        ParallelRanges(emissionCount, stageThreads, [&](std::uint32_t begin, std::uint32_t end, unsigned t) {
+            for (std::uint32_t k{begin}; k < end && partBase[t] != 0; ++k) {
+                offsets[k + 1] += partBase[t];
+            }
+        });
     }
     if (Form(h) == g4b::kPlain) {
         std::uint32_t k{0};

@@ -197,3 +197,57 @@ def test_autotune_picks_a_valid_shape(scene, batch):
         host.relaunch()
         after = host.complete_oldest_batch()
     assert before.detections.tobytes() == after.detections.tobytes()
+
+
+def _events_slice(batch, first, last):
+    """The batch's events [first, last) with their gensteps (contiguous per event)."""
+    keep = (batch.emission_event_indices >= first) & (batch.emission_event_indices < last)
+    return PhotonTransportBatch(batch.emissions[keep], batch.event_ids[first:last],
+                                batch.emission_event_indices[keep] - first)
+
+
+def _without_time(statistics):
+    return {k: v for k, v in statistics.items() if k != "transport_time_ms"}
+
+
+def test_large_batches_are_staged_in_parallel_parts(scene):
+    """g4b_enqueue stages a batch of 2^17 gensteps or more with several host
+    threads: errors still name the first bad genstep in batch order, and the
+    staged batch (offsets summed across the parts) gives exactly the results of
+    its events enqueued in parts small enough for one thread."""
+    batch = scenes.workload("batched", event_count=7300, seed=21)
+    count = batch.emissions.shape[0]
+    assert count >= 2 ** 18  # four parts where the host has the threads
+    assert np.all(np.diff(batch.emission_event_indices.astype(np.int64)) >= 0)
+    early, late = count // 9, count - 3
+
+    def planted(fields):
+        emissions = batch.emissions.copy()
+        for (field, row), value in fields.items():
+            emissions[field][row] = value
+        return PhotonTransportBatch(emissions, batch.event_ids, batch.emission_event_indices)
+
+    with TransportHost(PhotonTransportConfig(seed=5)) as host:
+        with pytest.raises(ValueError, match="material"):
+            host.enqueue_emissions(scene, planted({("material_id", early): 9, ("volume_id", late): 77}))
+        with pytest.raises(ValueError, match="volume"):
+            host.enqueue_emissions(scene, planted({("volume_id", early): 77, ("material_id", late): 9}))
+        with pytest.raises(ValueError, match="volume"):
+            host.enqueue_emissions(scene, planted({("volume_id", late): 77}))
+        with pytest.raises(ValueError, match="does not match"):
+            host.enqueue_emissions(scene, planted({("event_id", late): 987654}))
+        host.enqueue_emissions(scene, batch)
+        whole = host.complete_oldest_batch()
+        whole.detections = whole.detections.copy()
+        parts = []
+        events = batch.event_ids.shape[0]
+        for first, last in ((0, events // 3), (events // 3, 2 * events // 3), (2 * events // 3, events)):
+            part = _events_slice(batch, first, last)
+            assert part.emissions.shape[0] < 2 ** 17  # one staging thread
+            host.enqueue_emissions(scene, part)
+            out = host.complete_oldest_batch()
+            parts.append((out.detections.copy(), out.event_statistics))
+    assert whole.statistics["detected_count"] > 0
+    assert whole.detections.tobytes() == np.concatenate([d for d, _ in parts]).tobytes()
+    assert [(e, _without_time(s)) for e, s in whole.event_statistics] == \
+        [(e, _without_time(s)) for _, stats in parts for e, s in stats]
