@@ -1048,11 +1048,13 @@ void Stage(g4b_handle& h, const g4b_optical_emission* emissions, std::uint32_t e
     std::vector<std::vector<std::uint8_t>> hasEmissionBy(tallyThreads);
     std::vector<std::uint64_t> photonsBy(tallyThreads, 0);
     std::vector<std::uint8_t> mismatchBy(tallyThreads, 0);
+    for (unsigned t{}; t < tallyThreads; ++t) {  // allocated here: the parts must not throw
+        capturedBy[t].assign(eventCount, 0);
+        hasEmissionBy[t].assign(eventCount, 0);
+    }
     ParallelRanges(emissionCount, tallyThreads, [&](std::uint32_t begin, std::uint32_t end, unsigned t) {
         std::vector<std::uint64_t>& captured{capturedBy[t]};
         std::vector<std::uint8_t>& hasEmission{hasEmissionBy[t]};
-        captured.assign(eventCount, 0);
-        hasEmission.assign(eventCount, 0);
         std::uint64_t photons{0};
         for (std::uint32_t i{begin}; i < end; ++i) {
             const auto index{emissionEventIndices[i]};
