@@ -125,3 +125,27 @@ def test_synthetic_gensteps_are_seeded_and_well_formed(engine_lib):
     # uneven events: tens to ~1e5 photons
     per_event = np.bincount(a.emission_event_indices, weights=a.emissions["photon_count"], minlength=300)
     assert per_event.max() > 50 * max(per_event.min(), 1)
+
+
+def test_event_statistics_read_as_the_list_of_the_records():
+    """complete_oldest_batch returns g4b_event_statistics records as an
+    EventStatisticsList: the [(event_id, statistics dict)] list, in batch order,
+    built on first read with the same Python types as a field-by-field read."""
+    from g4go_b200 import _abi, transport
+
+    records = (_abi.EventStatistics * 5)()
+    for i in range(5):
+        records[i].event_id = 100 + 7 * i
+        records[i].statistics.valid_fields = 0x3ff
+        records[i].statistics.detected_count = 2 ** 40 + i
+        records[i].statistics.transport_time_ms = 0.25 * i
+    expected = [(int(r.event_id), transport._stats_dict(r.statistics)) for r in records[:4]]
+    view = transport._event_statistics(records, 4)
+    assert len(view) == 4
+    assert view == expected and expected == list(view)
+    assert view[0] == expected[0] and view[-1][0] == 121 and view[1:3] == expected[1:3]
+    assert [e for e, _ in view] == [100, 107, 114, 121]
+    assert type(view[3][1]["detected_count"]) is int and type(view[3][1]["transport_time_ms"]) is float
+    assert view == transport._event_statistics(records, 4)
+    assert view != transport._event_statistics(records, 5)
+    assert transport._event_statistics(records, 0) == []
