@@ -18,6 +18,7 @@
 // itself, converted by g4b::BoxScene (g4b_scene_adapter.hpp).
 #pragma once
 
+#include <algorithm>
 #include <cstddef>
 #include <cstdint>
 #include <memory>
@@ -105,6 +106,7 @@ public:
         Check(g4b_enqueue(fHandle, reinterpret_cast<const g4b_optical_emission*>(batch.emissions.data()),
                           static_cast<std::uint32_t>(batch.emissions.size()), batch.eventIDs.data(),
                           static_cast<std::uint32_t>(batch.eventIDs.size()), batch.emissionEventIndices.data()));
+        fPendingEvents = static_cast<std::uint32_t>(batch.eventIDs.size());
     }
 
     TransportOutput CompleteOldestBatch() {
@@ -125,6 +127,34 @@ public:
         return output;
     }
 
+    // CompleteOldestBatch into the caller's detection buffer, without asking
+    // for the counts first. With a pinned buffer (g4b_host_alloc), a batch of
+    // at least 2^24 photons has each wave's detections copied into it while
+    // its later waves still run. The batch's records are the first
+    // `detectionCount` of `detections`; `output.detections` stays empty.
+    // Returns false, with the batch still pending, when `capacity` is below
+    // the batch's detection count: CompleteOldestBatch() then completes it.
+    bool CompleteOldestBatchInto(g4b_photon_detection* detections, std::uint64_t capacity, TransportOutput& output,
+                                 std::uint64_t& detectionCount) {
+        output.detections.clear();
+        output.eventStatistics.resize(std::max<std::uint32_t>(fPendingEvents, 1U));
+        g4b_output raw{};
+        raw.detections = detections;
+        raw.detection_capacity = capacity;
+        raw.event_statistics = output.eventStatistics.data();
+        raw.event_capacity = fPendingEvents;
+        const int status{g4b_complete(fHandle, &raw)};
+        if (status == G4B_ERR_CAPACITY) {
+            return false;
+        }
+        Check(status);
+        output.eventStatistics.resize(raw.event_count);
+        output.statistics = raw.statistics;
+        output.performance = raw.performance;
+        detectionCount = raw.detection_count;
+        return true;
+    }
+
     g4b_handle* Handle() const { return fHandle; }
 
 private:
@@ -135,6 +165,7 @@ private:
     }
 
     g4b_handle* fHandle{nullptr};
+    std::uint32_t fPendingEvents{0};  // events of the batch last enqueued
     const void* fSceneAddress{nullptr};
     std::unique_ptr<BoxScene> fBoxScene;
 };
