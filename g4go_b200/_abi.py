@@ -118,7 +118,8 @@ class Config(C.Structure):
         ("use_cuda_graph", C.c_uint32),
         ("record_photon_fates", C.c_uint32),
         ("generation_pass", C.c_uint32),
-        ("reserved", C.c_uint32 * 6),
+        ("wave_photons", C.c_uint32),
+        ("reserved", C.c_uint32 * 5),
     ]
 
 
@@ -371,7 +372,7 @@ class SynthParams(C.Structure):
     ]
 
 
-# Every symbol include/g4b.h and include/g4b_synth.h declare, with its ctypes signature.
+# Every symbol include/g4b.h and include/g4b_scheduler.h declare (libg4b.so), with its ctypes signature.
 _VP = C.c_void_p
 _U32 = C.c_uint32
 _U64 = C.c_uint64
@@ -414,6 +415,9 @@ SIGNATURES = {
     "g4b_scheduler_destroy": (_I32, [_VP]),
     "g4b_scheduler_replay": (_I32, [_VP, _VP, _PU64, _PU32, _U32, _U32, _U32, _PU64, _PD]),
     "g4b_scheduler_last_error": (C.c_char_p, []),
+}
+# Every symbol include/g4b_synth.h declares (libg4b_synth.so).
+SYNTH_SIGNATURES = {
     "g4b_synth_electrons": (_I32, [C.POINTER(SynthParams), C.POINTER(_VP)]),
     "g4b_synth_isotropic_photons": (
         _I32,
@@ -429,6 +433,7 @@ SIGNATURES = {
 
 _lock = threading.Lock()
 _lib: C.CDLL | None = None
+_synth: C.CDLL | None = None
 
 
 def library_path() -> Path:
@@ -456,6 +461,29 @@ def load() -> C.CDLL:
         if lib.g4b_abi_version() != ABI_VERSION:
             raise ImportError("libg4b.so ABI version does not match the Python binding")
         _lib = lib
+        return lib
+
+
+def load_synth() -> C.CDLL:
+    """Loads the seeded genstep source (libg4b_synth.so), building it first if
+    it is missing or stale. It needs no GPU and does not load the engine."""
+    global _synth
+    with _lock:
+        if _synth is not None:
+            return _synth
+        try:
+            path = _build.build_synth()
+        except Exception as error:
+            if _build.SYNTH_LIBRARY.exists():
+                path = _build.SYNTH_LIBRARY
+            else:
+                raise ImportError(f"the genstep source library is missing and cannot be built: {error}") from error
+        lib = C.CDLL(str(path))
+        for name, (restype, argtypes) in SYNTH_SIGNATURES.items():
+            function = getattr(lib, name)
+            function.restype = restype
+            function.argtypes = argtypes
+        _synth = lib
         return lib
 
 

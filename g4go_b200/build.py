@@ -20,17 +20,22 @@ LIBRARY = LIB_DIR / "libg4b.so"
 SOURCES = [
     PACKAGE / "csrc" / "transport_kernels.cu",
     PACKAGE / "csrc" / "engine.cpp",
-    PACKAGE / "csrc" / "synth.cpp",
     PACKAGE / "csrc" / "scheduler.cpp",
 ]
 HEADERS = [
     PACKAGE / "csrc" / "g4b_device.cuh",
+    PACKAGE / "csrc" / "g4b_dual.cuh",
     PACKAGE / "csrc" / "engine_layout.h",
     PACKAGE / "csrc" / "kernels.h",
     PACKAGE.parent / "include" / "g4b.h",
-    PACKAGE.parent / "include" / "g4b_synth.h",
     PACKAGE.parent / "include" / "g4b_scheduler.h",
 ]
+# The seeded genstep source that stands in for Geant4 in tests and the
+# benchmark: host code only, in a library of its own, so that neither the
+# engine carries it nor a CPU-only run (the oracle's timing) loads the engine.
+SYNTH_LIBRARY = LIB_DIR / "libg4b_synth.so"
+SYNTH_SOURCES = [PACKAGE / "csrc" / "synth.cpp"]
+SYNTH_HEADERS = [PACKAGE.parent / "include" / "g4b_synth.h", PACKAGE.parent / "include" / "g4b.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -44,14 +49,29 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found: the CUDA toolkit is required to build the engine")
 
 
-def needs_build() -> bool:
-    if not LIBRARY.exists():
+def needs_build(library: Path = LIBRARY, inputs=None) -> bool:
+    if not library.exists():
         return True
-    built = LIBRARY.stat().st_mtime
-    return any(path.stat().st_mtime > built for path in SOURCES + HEADERS + [Path(__file__)])
+    built = library.stat().st_mtime
+    inputs = SOURCES + HEADERS if inputs is None else inputs
+    return any(path.stat().st_mtime > built for path in list(inputs) + [Path(__file__)])
+
+
+def build_synth(force: bool = False) -> Path:
+    """libg4b_synth.so from synth.cpp with the host compiler (no CUDA)."""
+    if not force and not needs_build(SYNTH_LIBRARY, SYNTH_SOURCES + SYNTH_HEADERS):
+        return SYNTH_LIBRARY
+    LIB_DIR.mkdir(parents=True, exist_ok=True)
+    temporary = SYNTH_LIBRARY.with_suffix(".so.tmp")
+    command = [os.environ.get("CXX", "g++"), "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-shared",
+               "-o", str(temporary), *map(str, SYNTH_SOURCES), "-lpthread"]
+    subprocess.run(command, check=True, cwd=PACKAGE)
+    os.replace(temporary, SYNTH_LIBRARY)
+    return SYNTH_LIBRARY
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
+    build_synth(force=force)
     if not force and not needs_build():
         return LIBRARY
     LIB_DIR.mkdir(parents=True, exist_ok=True)

@@ -38,6 +38,7 @@ using g4b::EventCounters;
 using g4b::HitColumns;
 using g4b::kInvalidID;
 using g4b::LaunchParams;
+using g4b::kWaveSlots;
 using g4b::PackedProperty;
 using g4b::PackedScene;
 using g4b::RunCounters;
@@ -171,20 +172,35 @@ struct g4b_handle {
     DeviceBuffer dHits[kHitColumns];
     std::uint64_t hitCapacity{0};
     DeviceBuffer dBitmap, dPrefix, dBlockSums, dDetections, dFate, dFateTime, dGradient;
-    DeviceBuffer dStore;    // two photon stores of the generation pass (waves alternate)
-    DeviceBuffer dTickets;  // the two waves' device work tickets
+    // kWaveSlots photon stores and work tickets of the generation pass: wave k
+    // uses slot k % kWaveSlots, and its transport runs on transport stream
+    // k % kWaveSlots (the handle's stream, then waveStreams). Up to kWaveSlots
+    // waves are in flight, so a wave's longest photon histories - serial
+    // chains of thousands of steps - overlap the next waves' transports
+    // instead of holding up the GPU.
+    DeviceBuffer dStore;
+    DeviceBuffer dTickets;
+    DeviceBuffer dDeferred;        // per slot: kDeferredCapacity parked long histories
+    DeviceBuffer dDeferredCounts;  // per slot: how many were parked
     cudaStream_t generationStream{nullptr};
+    cudaStream_t waveStreams[kWaveSlots - 1]{};
     cudaEvent_t zeroedEvent{nullptr};
-    cudaEvent_t generatedEvent[2]{};
-    cudaEvent_t storeFreeEvent[2]{};
+    cudaEvent_t generatedEvent[kWaveSlots]{};
+    cudaEvent_t storeFreeEvent[kWaveSlots]{};
+    cudaEvent_t orderedEvent[2]{};  // a wave's ordering done (the next wave's ordering follows it)
+    cudaEvent_t joinEvents[kWaveSlots - 1]{};  // each wave stream's last work, joined into the handle's stream
     cudaGraphExec_t wavesExec{nullptr};  // the generation-pass waves of the last batch, captured
-    // Per-wave ordering of the generation-pass form: after each wave's
-    // transport its hits are ordered into dDetections on the same stream, the
-    // hit-row counts before and after each wave kept in dWaveRows (copied to
-    // hWaveRows) and an event recorded, so g4b_complete can copy each wave's
+    // Per-wave hits and ordering of the generation-pass form: wave k writes its
+    // hits to rows [k * waveRegionRows, (k + 1) * waveRegionRows) of the hit
+    // buffer, counting them in dWaveCounts[k]; after its transport they are
+    // ordered into dDetections from row dWaveRows[k] on (the sum of the earlier
+    // waves' counts, chained on the device), dWaveRows[k + 1] copied to
+    // hWaveRows and an event recorded, so g4b_complete can copy each wave's
     // detections to the host while later waves run.
+    DeviceBuffer dWaveCounts;
     DeviceBuffer dWaveRows;
     PinnedBuffer hWaveRows;
+    std::uint64_t waveRegionRows{0};
     std::vector<cudaEvent_t> waveEvents;
     std::uint64_t pendingWaves{0};  // waves of the pending batch ordered that way (0: none)
     cudaStream_t copyStream{nullptr};
@@ -237,11 +253,17 @@ int Form(const g4b_handle& h) { return h.config.launch_form == G4B_FORM_PLAIN ? 
 // generation inside the transport loop (2). A batch below
 // kGenerationPassMinPhotons keeps generation in the loop: a single wave has
 // nothing to overlap its generation with, and the transport of a small batch
-// is bound by its tail, so the pass only adds latency there.
+// is bound by its tail, so the pass only adds latency there. Config 3 takes
+// the pass for a batch of any size (the same kernels as a large batch's).
 constexpr std::uint64_t kGenerationPassMinPhotons{1ULL << 24};
 bool UsesGenerationPass(const g4b_handle& h) {
-    return Form(h) == g4b::kBatched && Precision(h) == g4b::kFP32 && h.config.generation_pass != 2U &&
-           h.photonCount >= kGenerationPassMinPhotons;
+    if (Form(h) != g4b::kBatched || Precision(h) != g4b::kFP32 || h.photonCount == 0U) {
+        return false;
+    }
+    if (h.config.generation_pass == 3U) {
+        return true;
+    }
+    return h.config.generation_pass != 2U && h.photonCount >= kGenerationPassMinPhotons;
 }
 
 // The kernel variant of a form: with the coincidence counters only when
@@ -642,6 +664,7 @@ LaunchParams BaseParams(const g4b_handle& h) {
     hits.slot = h.dHits[11].As<std::uint32_t>();
     hits.capacity = h.hitCapacity;
     p.hits = hits;
+    p.hitCounter = &p.run->hitCount;
     p.photonFate = h.config.record_photon_fates != 0 ? h.dFate.As<std::uint32_t>() : nullptr;
     p.photonTime = h.config.record_photon_fates != 0 ? h.dFateTime.As<double>() : nullptr;
     return p;
@@ -721,9 +744,13 @@ void LaunchBatchedGraph(g4b_handle& h, const LaunchParams& params, unsigned grid
 }
 
 // Photons per wave of the generation pass: the batch cut into equal waves
-// of at most kPhotonStoreWave.
+// of at most kPhotonStoreWave, or of at most the configured wave_photons.
 std::uint64_t WavePhotons(const g4b_handle& h) {
-    const std::uint64_t waves{(h.photonCount + g4b::kPhotonStoreWave - 1U) / g4b::kPhotonStoreWave};
+    const std::uint64_t limit{h.config.wave_photons != 0U
+                                  ? std::min<std::uint64_t>((h.config.wave_photons + 31ULL) / 32ULL * 32ULL,
+                                                            g4b::kPhotonStoreWave)
+                                  : g4b::kPhotonStoreWave};
+    const std::uint64_t waves{(h.photonCount + limit - 1U) / limit};
     // a multiple of 32, so every wave starts on a word of the slot bitmap
     return waves == 0U ? 0U : ((h.photonCount + waves - 1U) / waves + 31U) / 32U * 32U;
 }
@@ -769,25 +796,40 @@ void EnsureGenerationStream(g4b_handle& h) {
     }
     Check(cudaStreamCreateWithFlags(&h.generationStream, cudaStreamNonBlocking), "cudaStreamCreateWithFlags");
     Check(cudaEventCreateWithFlags(&h.zeroedEvent, cudaEventDisableTiming), "cudaEventCreate");
-    for (int k{}; k < 2; ++k) {
+    for (std::uint32_t k{}; k < kWaveSlots; ++k) {
         Check(cudaEventCreateWithFlags(&h.generatedEvent[k], cudaEventDisableTiming), "cudaEventCreate");
         Check(cudaEventCreateWithFlags(&h.storeFreeEvent[k], cudaEventDisableTiming), "cudaEventCreate");
+    }
+    for (std::uint32_t k{}; k + 1U < kWaveSlots; ++k) {
+        Check(cudaStreamCreateWithFlags(&h.waveStreams[k], cudaStreamNonBlocking), "cudaStreamCreateWithFlags");
+        Check(cudaEventCreateWithFlags(&h.joinEvents[k], cudaEventDisableTiming), "cudaEventCreate");
+    }
+    for (auto& event : h.orderedEvent) {
+        Check(cudaEventCreateWithFlags(&event, cudaEventDisableTiming), "cudaEventCreate");
     }
 }
 
 // Batched FP32 form with a generation pass. The batch is cut into equal waves
 // of at most kPhotonStoreWave photons. GeneratePhotons fills a wave's store
 // on the generation stream, and the transport kernel then takes the wave's
-// photons from it on the handle's stream. The two stores and work tickets
-// alternate, so wave k+1 is generated while wave k is transported: its blocks
-// fill the SMs that wave k's finished warps leave. Counters are zeroed once
-// per batch. Returns the number of kernels launched.
+// photons from it. The two stores and work tickets alternate, so wave k+1 is
+// generated while wave k is transported: its blocks fill the SMs that wave
+// k's finished warps leave. The transports alternate between two streams as
+// well, so wave k+1's transport also starts while wave k's last warps still
+// run their longest photon histories; each wave has its own region of the hit
+// buffer and its own row counter for that. The waves' orderings run in wave
+// order. Counters are zeroed once per batch. Returns the number of kernels
+// launched.
 void PrepareWaves(g4b_handle& h) {
     EnsureGenerationStream(h);
     const std::uint64_t wave{WavePhotons(h)};
     const std::uint64_t waves{(h.photonCount + wave - 1U) / wave};
-    h.dStore.Ensure(2U * StoreBytes(wave), "cudaMalloc photon stores");
-    h.dTickets.Ensure(2U * sizeof(unsigned int), "cudaMalloc work tickets");
+    h.dStore.Ensure(kWaveSlots * StoreBytes(wave), "cudaMalloc photon stores");
+    h.dTickets.Ensure(2U * kWaveSlots * sizeof(unsigned int), "cudaMalloc work tickets");  // waves, parked photons
+    h.dDeferred.Ensure(std::size_t{kWaveSlots} * g4b::kDeferredCapacity * sizeof(g4b::DeferredPhoton),
+                       "cudaMalloc deferred photons");
+    h.dDeferredCounts.Ensure(kWaveSlots * sizeof(unsigned int), "cudaMalloc deferred counts");
+    h.dWaveCounts.Ensure(waves * sizeof(unsigned long long), "cudaMalloc wave counts");
     h.dWaveRows.Ensure((waves + 1U) * sizeof(unsigned long long), "cudaMalloc wave rows");
     h.hWaveRows.Ensure((waves + 1U) * sizeof(unsigned long long), "cudaMallocHost wave rows");
     while (h.waveEvents.size() < waves) {
@@ -795,6 +837,8 @@ void PrepareWaves(g4b_handle& h) {
         Check(cudaEventCreateWithFlags(&event, cudaEventDisableTiming), "cudaEventCreate");
         h.waveEvents.push_back(event);
     }
+    // every wave gets an equal share of the hit rows
+    h.waveRegionRows = h.hitCapacity / waves;
     const std::uint32_t words{static_cast<std::uint32_t>((h.photonCount + 31U) / 32U)};
     h.dBitmap.Ensure(sizeof(std::uint32_t) * words, "cudaMalloc slot bitmap");
     h.dPrefix.Ensure(sizeof(std::uint32_t) * words, "cudaMalloc slot prefix");
@@ -802,66 +846,123 @@ void PrepareWaves(g4b_handle& h) {
     h.dDetections.Ensure(sizeof(g4b_photon_detection) * h.hitCapacity, "cudaMalloc detections");
 }
 
+// Rows [first, first + rows) of the hit buffer as columns of their own.
+HitColumns HitRegion(const HitColumns& hits, std::uint64_t first, std::uint64_t rows) {
+    HitColumns region{hits};
+    region.positionX += first;
+    region.positionY += first;
+    region.positionZ += first;
+    region.time += first;
+    region.directionX += first;
+    region.directionY += first;
+    region.directionZ += first;
+    region.energy += first;
+    region.eventID += first;
+    region.photonID += first;
+    region.sensorID += first;
+    region.slot += first;
+    region.capacity = rows;
+    return region;
+}
+
 std::uint64_t LaunchBatchedWaves(g4b_handle& h, const LaunchParams& base, unsigned grid, std::uint32_t block,
                                  bool capturing = false) {
     PrepareWaves(h);
     const std::uint64_t wave{WavePhotons(h)};
     const std::uint64_t waves{(h.photonCount + wave - 1U) / wave};
+    auto* waveCounts{h.dWaveCounts.As<unsigned long long>()};
+    auto* waveRows{h.dWaveRows.As<unsigned long long>()};
     const auto waveParams{[&](std::uint64_t k) {
         LaunchParams p{base};
         p.photonBegin = static_cast<std::uint32_t>(k * wave);
         p.photonEnd = static_cast<std::uint32_t>(std::min<std::uint64_t>((k + 1U) * wave, h.photonCount));
-        p.store = StoreView(h, wave, static_cast<int>(k % 2U));
-        p.workTicket = h.dTickets.As<unsigned int>() + k % 2U;
+        p.store = StoreView(h, wave, static_cast<int>(k % kWaveSlots));
+        p.workTicket = h.dTickets.As<unsigned int>() + k % kWaveSlots;
+        p.hits = HitRegion(base.hits, k * h.waveRegionRows, h.waveRegionRows);
+        p.hitCounter = waveCounts + k;
+        p.deferred.photons = h.dDeferred.As<g4b::DeferredPhoton>() + (k % kWaveSlots) * g4b::kDeferredCapacity;
+        p.deferred.count = h.dDeferredCounts.As<unsigned int>() + k % kWaveSlots;
+        p.deferred.capacity = g4b::kDeferredCapacity;
         return p;
     }};
+    cudaStream_t streams[kWaveSlots]{h.stream};
+    for (std::uint32_t k{1}; k < kWaveSlots; ++k) {
+        streams[k] = h.waveStreams[k - 1U];
+    }
     const unsigned generateGrid{static_cast<unsigned>(h.smCount) * 8U};
     Check(g4b::LaunchZeroCounters(base.events, base.eventCount, base.run, h.stream), "zero counters");
-    auto* waveRows{h.dWaveRows.As<unsigned long long>()};
+    Check(cudaMemsetAsync(waveCounts, 0, waves * sizeof(unsigned long long), h.stream), "zero wave counts");
     Check(cudaMemsetAsync(waveRows, 0, sizeof(unsigned long long), h.stream), "zero wave rows");
     Check(cudaEventRecord(h.zeroedEvent, h.stream), "cudaEventRecord");
     Check(cudaStreamWaitEvent(h.generationStream, h.zeroedEvent, 0), "cudaStreamWaitEvent");
+    for (cudaStream_t stream : h.waveStreams) {
+        Check(cudaStreamWaitEvent(stream, h.zeroedEvent, 0), "cudaStreamWaitEvent");
+    }
     Check(g4b::LaunchGenerate(waveParams(0), generateGrid, SceneSharedBytes(h), h.generationStream),
           "generation launch");
     Check(cudaEventRecord(h.generatedEvent[0], h.generationStream), "cudaEventRecord");
     std::uint64_t launches{2};
+    const bool ordered{h.config.ordered_detections != 0};
     for (std::uint64_t k{0}; k < waves; ++k) {
         const LaunchParams p{waveParams(k)};
-        Check(cudaStreamWaitEvent(h.stream, h.generatedEvent[k % 2U], 0), "cudaStreamWaitEvent");
-        Check(cudaMemsetAsync(p.workTicket, 0, sizeof(unsigned int), h.stream), "reset work ticket");
+        const std::uint32_t slot{static_cast<std::uint32_t>(k % kWaveSlots)};
+        const cudaStream_t stream{streams[slot]};
+        Check(cudaStreamWaitEvent(stream, h.generatedEvent[slot], 0), "cudaStreamWaitEvent");
+        Check(cudaMemsetAsync(p.workTicket, 0, sizeof(unsigned int), stream), "reset work ticket");
+        Check(cudaMemsetAsync(p.deferred.count, 0, sizeof(unsigned int), stream), "reset deferred count");
         Check(g4b::LaunchTransport(p, g4b::kFP32, KernelOf(h, g4b::kBatched) | g4b::kPregenerated, grid, block,
-                                   SharedBytes(h, g4b::kBatched, block), h.stream),
+                                   SharedBytes(h, g4b::kBatched, block), stream),
               "transport launch");
-        Check(cudaEventRecord(h.storeFreeEvent[k % 2U], h.stream), "cudaEventRecord");
-        ++launches;
-        // order this wave's hits while the next wave is generated
-        Check(cudaMemcpyAsync(waveRows + k + 1U, &base.run->hitCount, sizeof(unsigned long long),
-                              cudaMemcpyDeviceToDevice, h.stream),
-              "cudaMemcpyAsync wave rows");
-        const bool ordered{h.config.ordered_detections != 0};
-        Check(g4b::LaunchOrderWaveHits(base.hits, waveRows + k, p.photonBegin, p.photonEnd, h.dBitmap.As<std::uint32_t>(),
-                                       h.dPrefix.As<std::uint32_t>(), h.dBlockSums.As<std::uint32_t>(),
-                                       h.dDetections.pointer, ordered, static_cast<unsigned>(h.smCount) * 4U,
-                                       h.stream),
-              "wave hit ordering");
-        launches += ordered ? 5U : 1U;
-        Check(cudaMemcpyAsync(h.hWaveRows.As<unsigned long long>() + k + 1U, waveRows + k + 1U,
-                              sizeof(unsigned long long), cudaMemcpyDeviceToHost, h.stream),
-              "cudaMemcpyAsync wave rows to host");
-        // inside a capture the record must stay a real event record for the host to wait on
-        Check(capturing ? cudaEventRecordWithFlags(h.waveEvents[k], h.stream, cudaEventRecordExternal)
-                        : cudaEventRecord(h.waveEvents[k], h.stream),
-              "cudaEventRecord wave");
+        Check(cudaEventRecord(h.storeFreeEvent[slot], stream), "cudaEventRecord");
+        // the photons the wave parked (they left their volume, or their
+        // history grew long), transported by a second launch of the same
+        // kernel from the queue, with small queue grabs; the wave's ordering
+        // waits for it
+        LaunchParams parked{p};
+        parked.deferred.input = 1U;
+        parked.photonBegin = 0U;
+        parked.photonEnd = 0U;
+        parked.chunk = 32U;
+        parked.workTicket = h.dTickets.As<unsigned int>() + kWaveSlots + slot;
+        Check(cudaMemsetAsync(parked.workTicket, 0, sizeof(unsigned int), stream), "reset work ticket");
+        Check(g4b::LaunchTransport(parked, g4b::kFP32, KernelOf(h, g4b::kBatched) | g4b::kPregenerated, grid, block,
+                                   SharedBytes(h, g4b::kBatched, block), stream),
+              "parked photons launch");
+        launches += 2;
         if (k + 1U < waves) {
-            if (k >= 1U) {  // the next wave's store and ticket were last used by wave k - 1
-                Check(cudaStreamWaitEvent(h.generationStream, h.storeFreeEvent[(k + 1U) % 2U], 0),
-                      "cudaStreamWaitEvent");
+            const std::uint32_t next{static_cast<std::uint32_t>((k + 1U) % kWaveSlots)};
+            if (k + 1U >= kWaveSlots) {  // the next wave's store and ticket were last used kWaveSlots waves ago
+                Check(cudaStreamWaitEvent(h.generationStream, h.storeFreeEvent[next], 0), "cudaStreamWaitEvent");
             }
             Check(g4b::LaunchGenerate(waveParams(k + 1U), generateGrid, SceneSharedBytes(h), h.generationStream),
                   "generation launch");
-            Check(cudaEventRecord(h.generatedEvent[(k + 1U) % 2U], h.generationStream), "cudaEventRecord");
+            Check(cudaEventRecord(h.generatedEvent[next], h.generationStream), "cudaEventRecord");
             ++launches;
         }
+        // order this wave's hits after the previous wave's, while the next
+        // wave is generated and transported
+        if (k >= 1U) {
+            Check(cudaStreamWaitEvent(stream, h.orderedEvent[(k + 1U) % 2U], 0), "cudaStreamWaitEvent");
+        }
+        Check(g4b::LaunchOrderWaveHits(p.hits, waveCounts + k, waveRows + k, base.run, p.photonBegin, p.photonEnd,
+                                       h.dBitmap.As<std::uint32_t>(), h.dPrefix.As<std::uint32_t>(),
+                                       h.dBlockSums.As<std::uint32_t>(), h.dDetections.pointer, ordered,
+                                       static_cast<unsigned>(h.smCount) * 4U, stream),
+              "wave hit ordering");
+        launches += ordered ? 6U : 2U;
+        Check(cudaEventRecord(h.orderedEvent[k % 2U], stream), "cudaEventRecord");
+        Check(cudaMemcpyAsync(h.hWaveRows.As<unsigned long long>() + k + 1U, waveRows + k + 1U,
+                              sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream),
+              "cudaMemcpyAsync wave rows to host");
+        // inside a capture the record must stay a real event record for the host to wait on
+        Check(capturing ? cudaEventRecordWithFlags(h.waveEvents[k], stream, cudaEventRecordExternal)
+                        : cudaEventRecord(h.waveEvents[k], stream),
+              "cudaEventRecord wave");
+    }
+    // the other transport streams' last work joins the handle's stream
+    for (std::uint32_t k{}; k + 1U < kWaveSlots; ++k) {
+        Check(cudaEventRecord(h.joinEvents[k], h.waveStreams[k]), "cudaEventRecord");
+        Check(cudaStreamWaitEvent(h.stream, h.joinEvents[k], 0), "cudaStreamWaitEvent");
     }
     return launches;
 }
@@ -1262,7 +1363,15 @@ void WaitMetadata(g4b_handle& h) {
     }
     Check(cudaEventSynchronize(h.metadataReadyEvent), "cudaEventSynchronize metadata");
     const auto* run{h.hRun.As<RunCounters>()};
-    if (run->hitCount > h.hitCapacity) {
+    if (h.pendingWaves != 0U) {
+        // generation-pass waves: each wave has an equal region of the hit rows
+        if (run->maxWaveHits > h.waveRegionRows) {
+            const std::uint64_t region{run->maxWaveHits + run->maxWaveHits / 8U};
+            EnsureHitCapacity(h, region * h.pendingWaves);
+            RunStaged(h);
+            Check(cudaEventSynchronize(h.metadataReadyEvent), "cudaEventSynchronize metadata");
+        }
+    } else if (run->hitCount > h.hitCapacity) {
         EnsureHitCapacity(h, run->hitCount + run->hitCount / 8U);
         RunStaged(h);
         Check(cudaEventSynchronize(h.metadataReadyEvent), "cudaEventSynchronize metadata");
@@ -1321,9 +1430,10 @@ void FillStatistics(const g4b_handle& h, g4b_output& output) {
 // (the generation-pass form): each wave's records are copied to a pinned
 // caller buffer as soon as that wave has finished, on the copy stream, while
 // the later waves still run; a pageable buffer gets them in one copy at the
-// end. Returns false when they cannot come from there (the device hit buffer
-// overflowed and the batch will rerun, or the caller's buffer is too small):
-// the whole-batch path then takes over.
+// end. Returns false when they cannot come from there (a wave's region of the
+// hit buffer overflowed and the batch was rerun, or the caller's buffer is too
+// small): the caller's completion then copies the rerun's records or reports
+// the capacity.
 bool CompleteByWaves(g4b_handle& h, g4b_output& output) {
     if (h.pendingWaves == 0U || output.detections == nullptr || output.detection_capacity == 0U) {
         return false;
@@ -1365,7 +1475,10 @@ bool CompleteByWaves(g4b_handle& h, g4b_output& output) {
     }
     Check(cudaEventRecord(h.hitsTimer.stop, h.copyStream), "cudaEventRecord");
     Check(cudaStreamSynchronize(h.copyStream), "cudaStreamSynchronize");
-    WaitMetadata(h);  // every wave has finished without overflow: no rerun happens here
+    // reruns the batch if a wave's region of the hit buffer overflowed; the
+    // records copied above are then incomplete and the caller's completion
+    // copies the rerun's instead
+    WaitMetadata(h);
     return h.hRun.As<RunCounters>()->hitCount == copied;
 }
 
@@ -1401,14 +1514,18 @@ void Complete(g4b_handle& h, g4b_output& output) {
             h.dPrefix.Ensure(sizeof(std::uint32_t) * words, "cudaMalloc slot prefix");
             h.dBlockSums.Ensure(sizeof(std::uint32_t) * ((words + 1023U) / 1024U + 1U), "cudaMalloc block sums");
         }
-        h.dDetections.Ensure(sizeof(g4b_photon_detection) * hits, "cudaMalloc detections");
-        const LaunchParams p{BaseParams(h)};
         const auto hostStart{std::chrono::steady_clock::now()};
-        Check(g4b::LaunchOrderHits(p.hits, hits, static_cast<std::uint32_t>(h.photonCount), h.dBitmap.As<std::uint32_t>(),
-                                   h.dPrefix.As<std::uint32_t>(), h.dBlockSums.As<std::uint32_t>(), h.dDetections.pointer,
-                                   ordered, h.stream),
-              "hit ordering");
-        h.launchCount += ordered ? 5 : 1;
+        if (h.pendingWaves == 0U) {
+            h.dDetections.Ensure(sizeof(g4b_photon_detection) * hits, "cudaMalloc detections");
+            const LaunchParams p{BaseParams(h)};
+            Check(g4b::LaunchOrderHits(p.hits, hits, static_cast<std::uint32_t>(h.photonCount),
+                                       h.dBitmap.As<std::uint32_t>(), h.dPrefix.As<std::uint32_t>(),
+                                       h.dBlockSums.As<std::uint32_t>(), h.dDetections.pointer, ordered, h.stream),
+                  "hit ordering");
+            h.launchCount += ordered ? 5 : 1;
+        }
+        // else: generation-pass waves, already ordered into dDetections by the
+        // (re)run that WaitMetadata waited for; only the copy remains
         Check(cudaEventRecord(h.hitsTimer.start, h.stream), "cudaEventRecord");
         cudaPointerAttributes attributes{};
         const bool pinnedTarget{cudaPointerGetAttributes(&attributes, output.detections) == cudaSuccess &&
@@ -1561,6 +1678,9 @@ int g4b_create(const g4b_config* config, g4b_handle** outHandle) {
         if (config->block_size != 0 && (config->block_size % 32 != 0 || config->block_size > 256)) {
             Throw(G4B_ERR_INVALID_ARGUMENT, "block_size must be a multiple of 32 and at most 256");
         }
+        if (config->generation_pass > 3U) {
+            Throw(G4B_ERR_INVALID_ARGUMENT, "generation_pass must be 0, 1, 2 or 3");
+        }
         SelectDevice(config->device);
         auto handle{std::make_unique<g4b_handle>()};
         handle->config = *config;
@@ -1610,8 +1730,20 @@ int g4b_destroy(g4b_handle* handle) {
     if (handle->metadataReadyEvent != nullptr) {
         cudaEventDestroy(handle->metadataReadyEvent);
     }
-    for (cudaEvent_t event : {handle->zeroedEvent, handle->generatedEvent[0], handle->generatedEvent[1],
-                              handle->storeFreeEvent[0], handle->storeFreeEvent[1]}) {
+    for (cudaStream_t stream : handle->waveStreams) {
+        if (stream != nullptr) {
+            cudaStreamSynchronize(stream);
+        }
+    }
+    std::vector<cudaEvent_t> events{handle->zeroedEvent, handle->orderedEvent[0], handle->orderedEvent[1]};
+    for (std::uint32_t k{}; k < kWaveSlots; ++k) {
+        events.push_back(handle->generatedEvent[k]);
+        events.push_back(handle->storeFreeEvent[k]);
+    }
+    for (cudaEvent_t event : handle->joinEvents) {
+        events.push_back(event);
+    }
+    for (cudaEvent_t event : events) {
         if (event != nullptr) {
             cudaEventDestroy(event);
         }
@@ -1622,6 +1754,11 @@ int g4b_destroy(g4b_handle* handle) {
     if (handle->copyStream != nullptr) {
         cudaStreamSynchronize(handle->copyStream);
         cudaStreamDestroy(handle->copyStream);
+    }
+    for (cudaStream_t stream : handle->waveStreams) {
+        if (stream != nullptr) {
+            cudaStreamDestroy(stream);
+        }
     }
     if (handle->generationStream != nullptr) {
         cudaStreamDestroy(handle->generationStream);

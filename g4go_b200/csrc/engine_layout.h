@@ -130,6 +130,9 @@ struct EventCounters {
 };
 
 // Batch-wide counters that have no per-event breakdown, plus queue state.
+// With a generation pass each wave counts its hit rows separately (its own
+// region of the hit buffer); hitCount is then their sum, and maxWaveHits the
+// largest, which tells whether a region overflowed.
 struct RunCounters {
     unsigned long long totalBounces;
     unsigned long long coincidentTraces;
@@ -137,7 +140,8 @@ struct RunCounters {
     unsigned long long hitCount;
     unsigned int workTicket;
     unsigned int reserved0;
-    unsigned long long reserved[3];
+    unsigned long long maxWaveHits;
+    unsigned long long reserved[2];
 };
 
 // Sums of the gradient replay over the detected photons, FP64. Parameter j:
@@ -182,6 +186,39 @@ struct PhotonStore {
 };
 constexpr std::uint32_t kPhotonStoreBytes{10U * 4U + 8U + 4U * 4U};  // per photon: 64
 constexpr std::uint32_t kPhotonStoreWave{1U << 26};                  // most photons in one generation wave
+constexpr std::uint32_t kWaveSlots{4};                                // generation-pass waves in flight at once
+
+// A photon of the generation pass's transport parked for the wave's
+// FinishDeferred kernel: the state StepPhoton continues from. Parked are the
+// photons that leave their volume the way the reference lets them (a trace
+// that has to search the whole scene; some then reflect totally at every step
+// for thousands of steps) and any history that reaches kDeferBounces bounces.
+// In the transport kernel such a photon would advance one step per Fresnel
+// ring completion and keep a whole block resident for one warp while the next
+// wave waits for its SMs.
+struct DeferredPhoton {
+    float position[3];
+    float direction[3];
+    float polarization[3];
+    float energy;
+    double time;
+    std::uint32_t volume;
+    std::uint32_t bounce;
+    std::uint32_t eventID;
+    std::uint32_t photonID;
+    std::uint32_t eventIndex;
+    std::uint32_t slot;
+};
+static_assert(sizeof(DeferredPhoton) == 72, "deferred photon layout");
+
+struct DeferredQueue {
+    DeferredPhoton* photons;  // nullptr: no deferral
+    unsigned int* count;      // photons parked; may exceed capacity (those beyond stay in their lane)
+    std::uint32_t capacity;
+    std::uint32_t input;      // 1: the launch transports the parked photons instead of the store's
+};
+constexpr std::uint32_t kDeferBounces{256};
+constexpr std::uint32_t kDeferredCapacity{1U << 19};  // per wave in flight (38 MB each)
 
 struct LaunchParams {
     const float4* emissions;               // [emissionCount] 128-byte gensteps as 8 float4 each
@@ -204,10 +241,12 @@ struct LaunchParams {
     EventCounters* events;
     RunCounters* run;
     HitColumns hits;
+    unsigned long long* hitCounter;        // allocator of hit rows: &run->hitCount, or a wave's own counter
     std::uint32_t* photonFate;             // optional [photons]
     double* photonTime;                    // optional [photons]
     PhotonStore store;                     // batched FP32 form with a generation pass
     unsigned int* workTicket;              // batched form: next unclaimed photon of the launch
+    DeferredQueue deferred;                // generation pass: where long histories are parked
 };
 
 }  // namespace g4b

@@ -46,12 +46,18 @@ cudaError_t LaunchOrderHits(const HitColumns& hits, unsigned long long count, st
                             std::uint32_t* bitmap, std::uint32_t* prefix, std::uint32_t* blockSums,
                             void* detectionsOut, bool ordered, cudaStream_t stream);
 
-// Ordering of one wave's hits on the transport's stream: its hit rows are
-// [rows[0], rows[1]) (device memory, clamped to hits.capacity), its slots lie
-// in [slotBegin, slotEnd) (slotBegin a multiple of 32), and its records are
-// written to the same rows of detectionsOut, in slot order within the wave.
-// Five launches when ordered (after a bitmap-range clear), one otherwise.
-cudaError_t LaunchOrderWaveHits(const HitColumns& hits, const unsigned long long* rows, std::uint32_t slotBegin,
+// Ordering of one wave's hits, after its transport: the wave's hits are rows
+// [0, *count) of `region` (its own region of the hit buffer; a count above
+// region.capacity means the region overflowed and only its rows are read),
+// its slots lie in [slotBegin, slotEnd) (slotBegin a multiple of 32). The
+// wave's records go to detectionsOut from row outRows[0] on, in slot order
+// within the wave; outRows[1] = outRows[0] + the rows written, and run gets
+// the wave's count added to hitCount and folded into maxWaveHits. Calls for
+// consecutive waves must run in wave order (they share blockSums and chain
+// outRows). Six launches when ordered (after a bitmap-range clear), two
+// otherwise.
+cudaError_t LaunchOrderWaveHits(const HitColumns& region, const unsigned long long* count,
+                                unsigned long long* outRows, RunCounters* run, std::uint32_t slotBegin,
                                 std::uint32_t slotEnd, std::uint32_t* bitmap, std::uint32_t* prefix,
                                 std::uint32_t* blockSums, void* detectionsOut, bool ordered, unsigned grid,
                                 cudaStream_t stream);

@@ -121,7 +121,7 @@ __device__ __forceinline__ void WriteHits(bool write, const Photon<R>& photon, s
     const int leader{__ffs(static_cast<int>(mask)) - 1};
     unsigned long long base{};
     if (static_cast<int>(lane) == leader) {
-        base = atomicAdd(&p.run->hitCount, static_cast<unsigned long long>(__popc(mask)));
+        base = atomicAdd(p.hitCounter, static_cast<unsigned long long>(__popc(mask)));
     }
     base = __shfl_sync(kFullMask, base, leader);
     if (write) {
@@ -221,6 +221,50 @@ __device__ __forceinline__ bool LoadStoredPhoton(const PhotonStore& store, std::
     photon.slot = slot;
     photon.bounce = 0U;
     return true;
+}
+
+// Parks a photon whose history reached kDeferBounces in the wave's queue for
+// FinishDeferred; false (the photon stays in its lane) when the queue is full.
+__device__ __forceinline__ bool DeferPhoton(const DeferredQueue& queue, const Photon<float>& photon) {
+    const unsigned int i{atomicAdd(queue.count, 1U)};
+    if (i >= queue.capacity) {
+        return false;
+    }
+    DeferredPhoton& parked{queue.photons[i]};
+    parked.position[0] = photon.position.x;
+    parked.position[1] = photon.position.y;
+    parked.position[2] = photon.position.z;
+    parked.direction[0] = photon.direction.x;
+    parked.direction[1] = photon.direction.y;
+    parked.direction[2] = photon.direction.z;
+    parked.polarization[0] = photon.polarization.x;
+    parked.polarization[1] = photon.polarization.y;
+    parked.polarization[2] = photon.polarization.z;
+    parked.energy = photon.energy;
+    parked.time = photon.time;
+    parked.volume = photon.volume;
+    parked.bounce = photon.bounce;
+    parked.eventID = photon.eventID;
+    parked.photonID = photon.photonID;
+    parked.eventIndex = photon.eventIndex;
+    parked.slot = photon.slot;
+    return true;
+}
+
+// Parked photon i back into a lane.
+__device__ __forceinline__ void LoadDeferredPhoton(const DeferredQueue& queue, std::uint32_t i, Photon<float>& photon) {
+    const DeferredPhoton& source{queue.photons[i]};
+    photon.position = {source.position[0], source.position[1], source.position[2]};
+    photon.direction = {source.direction[0], source.direction[1], source.direction[2]};
+    photon.polarization = {source.polarization[0], source.polarization[1], source.polarization[2]};
+    photon.energy = source.energy;
+    photon.time = source.time;
+    photon.volume = source.volume;
+    photon.bounce = source.bounce;
+    photon.eventID = source.eventID;
+    photon.photonID = source.photonID;
+    photon.eventIndex = source.eventIndex;
+    photon.slot = source.slot;
 }
 
 // Generation pass of the batched FP32 form: every photon of the wave
@@ -452,7 +496,11 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
     const unsigned lane{threadIdx.x & 31U};
     const unsigned lanesBelow{(1U << lane) - 1U};
     const R epsilon{R(p.epsilon)};
-    const std::uint32_t totalPhotons{p.photonEnd - p.photonBegin};
+    // the pass form's second launch per wave takes the photons the first one
+    // parked, and parks none itself
+    const bool fromQueue{kPregenerated && p.deferred.input != 0U};
+    const std::uint32_t totalPhotons{fromQueue ? min(*p.deferred.count, p.deferred.capacity)
+                                               : p.photonEnd - p.photonBegin};
     const std::uint32_t sceneEnd{(p.sceneBytes + 15U) & ~15U};
     // shared memory: scene, then one photon queue per warp (not with
     // kPregenerated: lanes take photons straight from the store), one Fresnel
@@ -539,7 +587,11 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
                 const std::uint32_t rank{static_cast<std::uint32_t>(__popc(need & lanesBelow))};
                 if (((need >> lane) & 1U) != 0U && rank < available) {
                     const std::uint32_t slot{chunkNext + rank};
-                    if (LoadStoredPhoton(p.store, slot - p.photonBegin, slot, photon)) {
+                    if (fromQueue) {
+                        LoadDeferredPhoton(p.deferred, slot - p.photonBegin, photon);
+                        counters.Switch(photon.eventIndex, p.events);
+                        alive = true;
+                    } else if (LoadStoredPhoton(p.store, slot - p.photonBegin, slot, photon)) {
                         counters.Switch(photon.eventIndex, p.events);
                         alive = true;
                     }
@@ -633,8 +685,31 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
         std::uint32_t result{kContinue};
         StepExtras extras{0U, 0U, 0U, 0U};
         FresnelJob<R> job;
+        // the pass form hands photons that leave their volume to the wave's
+        // FinishDeferred kernel while its queue has room (read once per warp
+        // iteration; a stale read only delays a hand-over by one step)
+        bool deferLeft{false};
+        if constexpr (kPregenerated) {
+            unsigned int parked{0U};
+            if (lane == 0U && p.deferred.photons != nullptr && !fromQueue) {
+                parked = *reinterpret_cast<volatile unsigned int*>(p.deferred.count);
+            }
+            parked = __shfl_sync(kFullMask, parked, 0);
+            deferLeft = p.deferred.photons != nullptr && !fromQueue && parked < p.deferred.capacity;
+        }
         if (alive) {
-            result = StepPhoton<R, true>(scene, pool, photon, p.seed, p.maxBounce, epsilon, extras, NoGradient(), &job);
+            result = StepPhoton<R, true>(scene, pool, photon, p.seed, p.maxBounce, epsilon, extras, NoGradient(), &job,
+                                         deferLeft);
+        }
+        if constexpr (kPregenerated) {
+            if (alive && result == kLeftVolume) {
+                // untouched by the step: handed over whole, or (queue full)
+                // stepped again next iteration with deferLeft false
+                if (DeferPhoton(p.deferred, photon)) {
+                    alive = false;
+                }
+                result = kContinue;
+            }
         }
         const bool parking{alive && result == kFresnelPending};
         const unsigned parkMask{__ballot_sync(kFullMask, parking)};
@@ -679,6 +754,14 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
                 counters.Finish(result, bounces);
                 tally.bounces += bounces;
                 RecordFate(p, photon.slot, result, bounces, photon.time);
+                alive = false;
+            }
+        }
+        if constexpr (kPregenerated) {
+            // a long history goes to the wave's FinishDeferred kernel, and the
+            // lane takes fresh work (identical results: the step is the same)
+            if (alive && photon.bounce >= kDeferBounces && p.deferred.photons != nullptr && !fromQueue &&
+                DeferPhoton(p.deferred, photon)) {
                 alive = false;
             }
         }
@@ -1055,37 +1138,49 @@ constexpr std::uint32_t kStaticScratchWords{kStaticStatusOffset + 64U};
 
 static __device__ __align__(256) std::uint32_t gStaticOrderScratch[kStaticScratchWords];
 
-// Marks each record's slot key in the bitmap. A key at or above slotLimit,
-// or one already marked, touches nothing and adds one to *status.
-// Per-wave ordering on the transport's stream: the wave's hit rows are
-// [rows[0], rows[1]) of the hit buffer (device-side counts, clamped to the
-// buffer's capacity), their slots lie in the wave's slot range, and the
-// records go to the same rows of the detection buffer, ranked within the wave.
-__global__ void MarkWaveSlots(const std::uint32_t* __restrict__ slots, const unsigned long long* __restrict__ rows,
-                              unsigned long long capacity, std::uint32_t* __restrict__ bitmap) {
-    const unsigned long long begin{min(rows[0], capacity)};
-    const unsigned long long end{min(rows[1], capacity)};
-    for (unsigned long long i = begin + blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x;
-         i < end; i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+// Per-wave ordering. Each wave of the generation pass writes its hits to its
+// own region of the hit buffer, rows [0, count) of the region (count is the
+// wave's row counter, clamped to the region's rows: a larger count means the
+// region overflowed and the batch reruns). The waves' records go to the
+// detection buffer one after another, in wave order: wave k's start row is
+// the sum of the earlier waves' counts, which AdvanceWaveRows computes on the
+// device once wave k's transport has finished, and the records are ranked by
+// slot within the wave.
+__global__ void AdvanceWaveRows(const unsigned long long* __restrict__ count, unsigned long long* __restrict__ outRows,
+                                unsigned long long regionRows, RunCounters* __restrict__ run) {
+    if (blockIdx.x == 0U && threadIdx.x == 0U) {
+        const unsigned long long c{*count};
+        outRows[1] = outRows[0] + min(c, regionRows);
+        run->hitCount += c;
+        run->maxWaveHits = max(run->maxWaveHits, c);
+    }
+}
+
+__global__ void MarkWaveSlots(const std::uint32_t* __restrict__ slots, const unsigned long long* __restrict__ count,
+                              unsigned long long regionRows, std::uint32_t* __restrict__ bitmap) {
+    const unsigned long long end{min(*count, regionRows)};
+    for (unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; i < end;
+         i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
         const std::uint32_t slot{slots[i]};
         atomicOr(bitmap + (slot >> 5U), 1U << (slot & 31U));
     }
 }
 
-__global__ void ScatterWaveDetections(const HitColumns hits, const unsigned long long* __restrict__ rows,
-                                      unsigned long long capacity, const std::uint32_t* __restrict__ bitmap,
+__global__ void ScatterWaveDetections(const HitColumns hits, const unsigned long long* __restrict__ count,
+                                      unsigned long long regionRows, const unsigned long long* __restrict__ outRows,
+                                      const std::uint32_t* __restrict__ bitmap,
                                       const std::uint32_t* __restrict__ prefix, bool ordered,
                                       float4* __restrict__ out) {
-    const unsigned long long begin{min(rows[0], capacity)};
-    const unsigned long long end{min(rows[1], capacity)};
-    for (unsigned long long i = begin + blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x;
-         i < end; i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
-        unsigned long long row{i};
+    const unsigned long long end{min(*count, regionRows)};
+    const unsigned long long first{outRows[0]};
+    for (unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; i < end;
+         i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+        unsigned long long row{first + i};
         if (ordered) {
             const std::uint32_t slot{hits.slot[i]};
             const std::uint32_t word{slot >> 5U};
             const std::uint32_t below{bitmap[word] & ((1U << (slot & 31U)) - 1U)};
-            row = begin + prefix[word] + static_cast<std::uint32_t>(__popc(below));
+            row = first + prefix[word] + static_cast<std::uint32_t>(__popc(below));
         }
         float4* record{out + row * 3ULL};
         record[0] = make_float4(hits.positionX[i], hits.positionY[i], hits.positionZ[i], hits.time[i]);
@@ -1095,6 +1190,8 @@ __global__ void ScatterWaveDetections(const HitColumns hits, const unsigned long
     }
 }
 
+// Marks each record's slot key in the bitmap. A key at or above slotLimit,
+// or one already marked, touches nothing and adds one to *status.
 __global__ void MarkKeysChecked(const std::uint32_t* __restrict__ keys, unsigned long long count,
                                 std::uint32_t slotLimit, std::uint32_t* __restrict__ bitmap,
                                 std::uint32_t* __restrict__ status) {
@@ -1298,10 +1395,12 @@ cudaError_t LaunchOrderHits(const HitColumns& hits, unsigned long long count, st
     return cudaGetLastError();
 }
 
-cudaError_t LaunchOrderWaveHits(const HitColumns& hits, const unsigned long long* rows, std::uint32_t slotBegin,
+cudaError_t LaunchOrderWaveHits(const HitColumns& region, const unsigned long long* count,
+                                unsigned long long* outRows, RunCounters* run, std::uint32_t slotBegin,
                                 std::uint32_t slotEnd, std::uint32_t* bitmap, std::uint32_t* prefix,
                                 std::uint32_t* blockSums, void* detectionsOut, bool ordered, unsigned grid,
                                 cudaStream_t stream) {
+    AdvanceWaveRows<<<1, 32, 0, stream>>>(count, outRows, region.capacity, run);
     if (ordered) {
         const std::uint32_t wordBegin{slotBegin / 32U};
         const std::uint32_t words{(slotEnd - slotBegin + 31U) / 32U};
@@ -1310,12 +1409,12 @@ cudaError_t LaunchOrderWaveHits(const HitColumns& hits, const unsigned long long
         if (error != cudaSuccess) {
             return error;
         }
-        MarkWaveSlots<<<grid, 256, 0, stream>>>(hits.slot, rows, hits.capacity, bitmap);
+        MarkWaveSlots<<<grid, 256, 0, stream>>>(region.slot, count, region.capacity, bitmap);
         BlockPopcount<<<blocks, 256, 0, stream>>>(bitmap + wordBegin, words, blockSums);
         ScanBlockSums<<<1, 1024, 0, stream>>>(blockSums, blocks);
         WordPrefix<<<blocks, 256, 0, stream>>>(bitmap + wordBegin, words, blockSums, prefix + wordBegin);
     }
-    ScatterWaveDetections<<<grid, 256, 0, stream>>>(hits, rows, hits.capacity, bitmap, prefix, ordered,
+    ScatterWaveDetections<<<grid, 256, 0, stream>>>(region, count, region.capacity, outRows, bitmap, prefix, ordered,
                                                     static_cast<float4*>(detectionsOut));
     return cudaGetLastError();
 }

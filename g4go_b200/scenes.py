@@ -132,12 +132,44 @@ def crystal_sipm_scene(params: DetectorParameters | None = None) -> Scene:
     return scene
 
 
+def rough_surface_scene(params: DetectorParameters | None = None) -> Scene:
+    """The detector with rough surfaces on the reference's bounded paths: a
+    ground unified wrapper (sigma_alpha 0.2 rad; specular lobe, spike,
+    backscatter and Lambertian parts) and a ground unified crystal-grease face
+    (sigma_alpha 0.1 rad, with a surface-roughness table so the roughness
+    criterion of the reference's dielectric surfaces runs). No glisur ground
+    surface: the reference's glisur facet loop never ends once a smear leaves
+    the unit ball."""
+    scene = crystal_sipm_scene(params)
+    energies = np.array([1.5, 4.5], np.float32)
+
+    def flat(value):
+        return energies, np.array([value, value], np.float32)
+
+    ground = scene.add_surface(Surface(
+        name="ground_wrapper", type=_abi.SURFACE_DIELECTRIC_METAL, model=_abi.MODEL_UNIFIED,
+        finish=_abi.FINISH_GROUND, model_value=0.2, reflectivity=flat(0.9),
+        specular_lobe=flat(0.3), specular_spike=flat(0.2), backscatter=flat(0.1),
+    ))
+    face = scene.add_surface(Surface(
+        name="ground_coupling", type=_abi.SURFACE_DIELECTRIC_DIELECTRIC, model=_abi.MODEL_UNIFIED,
+        finish=_abi.FINISH_GROUND, model_value=0.1, surface_roughness=flat(2.0e-5),
+        specular_lobe=flat(0.5), specular_spike=flat(0.3),
+    ))
+    scene.surface_bindings = [
+        SurfaceBinding(CRYSTAL, WORLD, ground),
+        SurfaceBinding(WORLD, CRYSTAL, SURF_COATING),
+        SurfaceBinding(CRYSTAL, GREASE, face),
+    ]
+    return scene
+
+
 # ---------------------------------------------------------------------------
 # Synthetic gensteps (include/g4b_synth.h)
 # ---------------------------------------------------------------------------
 
 def _take(batch_ptr: C.c_void_p) -> PhotonTransportBatch:
-    lib = _abi.load()
+    lib = _abi.load_synth()
     emissions = C.c_void_p()
     n = C.c_uint32()
     event_ids = C.c_void_p()
@@ -181,7 +213,7 @@ def electron_gensteps(
 ) -> PhotonTransportBatch:
     """Gensteps of `event_count` electrons entering the crystal's -z face."""
     p = params or DetectorParameters()
-    lib = _abi.load()
+    lib = _abi.load_synth()
     sp = _abi.SynthParams()
     sp.event_count = event_count
     sp.first_event_id = first_event_id
@@ -220,7 +252,7 @@ def isotropic_photons(
 ) -> PhotonTransportBatch:
     """Single photons uniform in the crystal, isotropic, wavelength uniform in the range."""
     p = params or DetectorParameters()
-    lib = _abi.load()
+    lib = _abi.load_synth()
     center = (C.c_float * 3)(0.0, 0.0, 0.0)
     half = (C.c_float * 3)(*p.crystal_half_mm)
     out = C.c_void_p()

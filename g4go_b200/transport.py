@@ -258,7 +258,10 @@ class PhotonTransportConfig:
     chunk_photons: int = 0
     use_cuda_graph: bool = True
     record_photon_fates: bool = False
-    generation_pass: int = 0  # batched FP32: 0/1 separate generation kernel, 2 generation inside the loop
+    # batched FP32: 0/1 separate generation kernel for batches of >= 2^24 photons,
+    # 2 generation inside the loop, 3 separate generation kernel at any size
+    generation_pass: int = 0
+    wave_photons: int = 0  # most photons per generation-pass wave (0: 2^26)
     device: int = -1
 
     def to_c(self) -> _abi.Config:
@@ -283,6 +286,7 @@ class PhotonTransportConfig:
         config.use_cuda_graph = int(bool(self.use_cuda_graph))
         config.record_photon_fates = int(bool(self.record_photon_fates))
         config.generation_pass = int(self.generation_pass)
+        config.wave_photons = int(self.wave_photons)
         return config
 
 
@@ -302,6 +306,24 @@ class PhotonTransportBatch:
     @property
     def photon_count(self) -> int:
         return int(self.emissions["photon_count"].sum(dtype=np.uint64))
+
+    def photon_slice(self, begin: int, end: int, ends: np.ndarray | None = None):
+        """The gensteps that hold flattened photon slots [begin, end) as a batch
+        of their own, with the slots' range inside it: (batch, (b, e)). Every
+        photon keeps its event ID and photon ID, and so its random numbers and
+        its history. `ends` (the cumulative photon counts, int64) may be passed
+        to save recomputing it for many slices."""
+        if ends is None:
+            ends = np.cumsum(self.emissions["photon_count"], dtype=np.int64)
+        total = int(ends[-1]) if ends.size else 0
+        if not 0 <= begin < end <= total:
+            raise ValueError(f"photon slice [{begin}, {end}) outside [0, {total})")
+        first = int(np.searchsorted(ends, begin, side="right"))
+        last = int(np.searchsorted(ends, end - 1, side="right")) + 1
+        events, local = np.unique(self.emission_event_indices[first:last], return_inverse=True)
+        part = PhotonTransportBatch(self.emissions[first:last], self.event_ids[events], local.astype(np.uint32))
+        offset = int(ends[first - 1]) if first > 0 else 0
+        return part, (begin - offset, end - offset)
 
 
 STAT_FIELDS = (
@@ -350,6 +372,19 @@ class EventStatisticsList(collections.abc.Sequence):
 
     def __repr__(self) -> str:
         return f"EventStatisticsList({self._list()!r})"
+
+
+def _check_detection_buffer(buffer) -> None:
+    """A caller's detection buffer must take g4b_complete's records in place:
+    the engine writes `capacity` 48-byte records from its first byte."""
+    if not isinstance(buffer, np.ndarray) or buffer.ndim != 1:
+        raise ValueError("detections_out must be a one-dimensional numpy array")
+    if buffer.dtype != DETECTION_DTYPE:
+        raise ValueError(f"detections_out must have the detection record dtype, not {buffer.dtype}")
+    if not buffer.flags.c_contiguous:
+        raise ValueError("detections_out must be C-contiguous (a strided view would be written across)")
+    if not buffer.flags.writeable:
+        raise ValueError("detections_out must be writeable")
 
 
 def _event_statistics(records, count: int) -> EventStatisticsList:
@@ -452,7 +487,12 @@ class TransportHost:
         """CompleteOldestBatch (OptiXTransportHost.cpp:779-883).
 
         counts_only: return statistics without copying the detections back
-        (they stay in device memory)."""
+        (they stay in device memory).
+        detections_out: a C-contiguous, writeable array of DETECTION_DTYPE
+        records (ValueError otherwise): the engine writes 48-byte records into
+        it by address."""
+        if detections_out is not None:
+            _check_detection_buffer(detections_out)
         if detections_out is not None and not counts_only and self._pending_batch is not None:
             # a caller buffer: complete at once, without first waiting for the
             # counts, so that a multi-wave batch's detections stream into it

@@ -214,8 +214,11 @@ typedef struct g4b_config {
                                         photons are made by a separate generation kernel into a photon
                                         store, in waves of up to 2^26 photons, and read by the transport
                                         kernel (smaller batches generate inside the transport loop);
-                                        2 -> always inside the transport loop */
-    uint32_t reserved[6];
+                                        2 -> always inside the transport loop;
+                                        3 -> always the separate generation kernel, whatever the size */
+    uint32_t wave_photons;           /* most photons in one generation-pass wave, rounded up to a multiple of
+                                        32; 0 -> 2^26. Smaller waves give a small batch several waves. */
+    uint32_t reserved[5];
 } g4b_config;
 
 /* --- Scene (analytic boxes) ------------------------------------------------

@@ -134,8 +134,14 @@ public:
     // `detectionCount` of `detections`; `output.detections` stays empty.
     // Returns false, with the batch still pending, when `capacity` is below
     // the batch's detection count: CompleteOldestBatch() then completes it.
+    // A null `detections` throws std::invalid_argument and leaves the batch
+    // pending (g4b_complete would otherwise take it as a counts-only call and
+    // leave the hits on the device).
     bool CompleteOldestBatchInto(g4b_photon_detection* detections, std::uint64_t capacity, TransportOutput& output,
                                  std::uint64_t& detectionCount) {
+        if (detections == nullptr) {
+            throw std::invalid_argument("CompleteOldestBatchInto needs a detection buffer");
+        }
         output.detections.clear();
         output.eventStatistics.resize(std::max<std::uint32_t>(fPendingEvents, 1U));
         g4b_output raw{};

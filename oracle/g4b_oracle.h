@@ -47,13 +47,21 @@ typedef struct oracle_result {
 /* Transports one batch. precision: G4B_PRECISION_FP32 or G4B_PRECISION_FP64.
  * threads: 0 -> all hardware threads. photon_begin/photon_end restrict the
  * run to a slice of the flattened photon range (photon_end 0 -> all), used
- * for bounded CPU-baseline samples. Returns 0 or a negative g4b_status. */
+ * for bounded CPU-baseline samples. Returns 0 or a negative g4b_status.
+ * With result->detections NULL the detections are kept (on the calling
+ * thread) for oracle_take_detections, so a caller that does not know the
+ * count in advance transports the photons once. */
 int oracle_transport(const g4b_scene* scene, const g4b_config* config, const g4b_optical_emission* emissions,
                      uint32_t emission_count, const uint32_t* event_ids, uint32_t event_count,
                      const uint32_t* emission_event_indices, uint32_t threads, uint64_t photon_begin,
                      uint64_t photon_end, oracle_result* result);
 
 const char* oracle_last_error(void);
+
+/* Copies up to `capacity` detections kept by the calling thread's last
+ * oracle_transport call without a detection buffer into `out`, releases them,
+ * and returns how many there were. */
+uint64_t oracle_take_detections(g4b_photon_detection* out, uint64_t capacity);
 
 /* Restated boundary functions (OptiXBoundaryPhysics.cuh), FP32 and FP64. */
 void oracle_fresnel_f(const float direction[3], const float polarization[3], const float normal[3], float index_from,
@@ -73,6 +81,20 @@ void oracle_sincos_turn_f(float turns, float* s, float* c);
 double oracle_log_d(double x);
 double oracle_exp_d(double x);
 void oracle_sincos_turn_d(double turns, double* s, double* c);
+
+/* GeneratePhoton (OptiXTransportDevice.cu:346-481) for photon local[i] of
+ * genstep emissionIndex[i], in FP32 or FP64. Each output row: position[3],
+ * direction[3], polarization[3], energy; the global time separately. */
+int oracle_generate(const g4b_scene* scene, uint64_t seed, uint32_t precision,
+                    const g4b_optical_emission* emissions, uint32_t emission_count, const uint32_t* emission_index,
+                    const uint32_t* local, uint32_t n, double* out, double* time_out);
+
+/* SampleProperty (OptiXTransportDevice.cu:198-216) on a property table, and
+ * SampleSpectrum (:322-344) on the CDF the oracle builds from a spectrum
+ * table (OptiXTransportHost.cpp:371-410), in FP32. */
+float oracle_sample_property_f(const float* energy, const float* values, uint32_t count, float x,
+                               float default_value);
+float oracle_sample_spectrum_f(const float* energy, const float* values, uint32_t count, float u);
 
 /* Uniform(seed, key, bounce, process, draw) (OptiXTransportDevice.cu:254-286). */
 float oracle_uniform_f(uint64_t seed, uint64_t photon_key, uint32_t bounce, uint32_t process, uint32_t draw);

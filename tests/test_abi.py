@@ -12,9 +12,9 @@ ROOT = Path(__file__).resolve().parent.parent
 HEADERS = sorted((ROOT / "include").glob("*.h"))
 
 
-def declared_functions():
+def declared_functions(headers=None):
     names = set()
-    for header in HEADERS:
+    for header in HEADERS if headers is None else headers:
         text = header.read_text()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         for match in re.finditer(r"^[A-Za-z_][\w\s\*]*?\b(g4b_\w+)\s*\(", text, flags=re.M):
@@ -23,13 +23,22 @@ def declared_functions():
 
 
 def test_every_declared_symbol_is_exported(engine_lib):
-    names = declared_functions()
+    """libg4b.so exports what g4b.h and g4b_scheduler.h declare; the genstep
+    source (g4b_synth.h) is a library of its own, and the engine carries none
+    of it."""
+    from g4go_b200 import _abi
+
+    synth_header = [h for h in HEADERS if h.name == "g4b_synth.h"]
+    names = declared_functions([h for h in HEADERS if h.name != "g4b_synth.h"])
     assert len(names) >= 20
     missing = [n for n in names if not hasattr(engine_lib, n)]
     assert not missing, missing
-    from g4go_b200 import _abi
-
     assert set(names) == set(_abi.SIGNATURES), "the ctypes binding must cover exactly the declared symbols"
+    synth_names = declared_functions(synth_header)
+    synth = _abi.load_synth()
+    assert synth_names and not [n for n in synth_names if not hasattr(synth, n)]
+    assert set(synth_names) == set(_abi.SYNTH_SIGNATURES)
+    assert not [n for n in synth_names if hasattr(engine_lib, n)]
 
 
 def test_record_layouts_match_the_reference(tmp_path):
@@ -149,3 +158,22 @@ def test_event_statistics_read_as_the_list_of_the_records():
     assert view == transport._event_statistics(records, 4)
     assert view != transport._event_statistics(records, 5)
     assert transport._event_statistics(records, 0) == []
+
+
+def test_caller_detection_buffers_are_checked_before_the_engine_writes():
+    """complete_oldest_batch(detections_out=...) hands the array's address to
+    g4b_complete, which writes 48-byte records: a wrong dtype, a strided view or
+    a read-only array must be refused before any engine call."""
+    import numpy as np
+
+    from g4go_b200 import transport
+
+    host = object.__new__(transport.TransportHost)  # no device here: the check comes first
+    good = np.empty(8, dtype=transport.DETECTION_DTYPE)
+    transport._check_detection_buffer(good)
+    readonly = np.empty(8, dtype=transport.DETECTION_DTYPE)
+    readonly.flags.writeable = False
+    for bad in (np.empty(8 * 48, dtype=np.uint8), np.empty(16, dtype=transport.DETECTION_DTYPE)[::2],
+                readonly, np.empty((2, 4), dtype=transport.DETECTION_DTYPE)):
+        with pytest.raises(ValueError):
+            host.complete_oldest_batch(detections_out=bad)

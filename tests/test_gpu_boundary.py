@@ -106,3 +106,32 @@ def test_device_uniform_bit_equal_to_oracle(oracle):
                      for k, b, p, d in zip(keys, bounce, process, draw)], dtype=np.float32)
     np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
     assert np.all((got > 0) & (got <= 1))
+
+
+def test_device_math_within_the_true_function_bounds():
+    """The device's own log / exp / sin+cos of turns (float), evaluated on the
+    GPU, against the true functions with the bounds tests/test_math_accuracy.py
+    states for the oracle's series."""
+    import test_math_accuracy as bounds
+
+    rng = np.random.default_rng(17)
+    x = bounds.log_arguments(rng)
+    bounds.check_log(x, eval_math("log", x))
+    x = bounds.exp_arguments(rng)
+    bounds.check_exp(x, eval_math("exp", x))
+    t = bounds.turn_arguments(rng)
+    s, c = eval_math("sincos_turn", t)
+    bounds.check_sincos(t, s, c)
+
+
+def test_device_uniform_is_the_reference_bit_for_bit():
+    """The device's counter RNG against the reference's own Uniform
+    (OptiXTransportDevice.cu:254-286, compiled for the host: the fixture of
+    tests/golden/make_golden_transport.py)."""
+    import reference_fixture as rf
+
+    golden = rf.load()
+    for s, seed in enumerate(golden["uniform_seeds"]):
+        got = eval_uniform(int(seed), golden["uniform_keys"], golden["uniform_bounce"], golden["uniform_process"],
+                           golden["uniform_draw"])
+        np.testing.assert_array_equal(got.view(np.uint32), golden["uniform"][s].view(np.uint32))

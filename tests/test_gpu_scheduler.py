@@ -4,7 +4,8 @@ Every photon's history depends only on its RNG counters (seed, event ID,
 photon ID), so an event's detections and statistics must not depend on which
 batch it lands in: events submitted one at a time from several threads, and
 batched by the scheduler however the timing falls, must come back bit for bit
-as in one direct batch of the same gensteps.
+as the CPU oracle transports the same gensteps in one batch, and as one
+direct engine batch of them.
 """
 import threading
 
@@ -24,23 +25,31 @@ COUNTERS = ("detected_count", "absorbed_count", "escaped_count", "truncated_coun
             "invalid_state_count", "zero_step_count")
 
 
+def split_by_event(out):
+    return {event_id: (out.detections[out.detections["event_id"] == event_id], stats)
+            for event_id, stats in out.event_statistics}
+
+
 @pytest.fixture(scope="module")
-def direct():
+def direct(oracle):
     scene = scenes.crystal_sipm_scene()
     batch = scenes.workload("batched", event_count=300, seed=3)
     with TransportHost(PhotonTransportConfig(seed=SEED)) as host:
         host.enqueue_emissions(scene, batch)
         out = host.complete_oldest_batch()
-    per_event = {}
-    for event_id, stats in out.event_statistics:
-        per_event[event_id] = (out.detections[out.detections["event_id"] == event_id], stats)
+    reference = oracle.transport(scene, batch, PhotonTransportConfig(seed=SEED, precision="fp32"))
+    per_event = split_by_event(reference)
+    engine = split_by_event(out)
+    for event_id, (detections, stats) in per_event.items():  # the direct batch is the oracle's too
+        assert engine[event_id][0].tobytes() == detections.tobytes(), event_id
+        assert all(engine[event_id][1][name] == stats[name] for name in COUNTERS), event_id
     submissions = [OpticalSubmission(int(event_id), batch.emissions[batch.emission_event_indices == i])
                    for i, event_id in enumerate(batch.event_ids)]
     return scene, submissions, per_event
 
 
 @pytest.mark.parametrize("serial", [False, True])
-def test_scheduled_events_match_one_direct_batch(direct, serial):
+def test_scheduled_events_match_the_oracle(direct, serial):
     scene, submissions, per_event = direct
     batching = BatchSchedulerConfig(target_photons_per_batch=1_500_000, batch_collection_timeout_ms=2, serial=serial)
     with OpticalBatchScheduler(PhotonTransportConfig(seed=SEED), scene, batching) as scheduler:

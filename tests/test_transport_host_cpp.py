@@ -5,8 +5,8 @@ The program defines the seven g4b_* functions the header calls. The stand-in
 engine stages a batch of four events and 12 detections, and its g4b_complete
 behaves as the engine's does: G4B_ERR_CAPACITY with the batch still pending when
 the detection buffer is too small, otherwise detections, counts and per-event
-records. The program checks CompleteOldestBatchInto (refused for a small
-buffer, then filled into the caller's buffer without a count query) and
+records. The program checks CompleteOldestBatchInto (refused for a null and
+for a small buffer, then filled into the caller's buffer without a count query) and
 CompleteOldestBatch (query first, then a vector of the exact size).
 """
 import subprocess
@@ -80,9 +80,11 @@ int main() {
     std::vector<g4b_photon_detection> buffer(16);
     g4b::TransportOutput output;
     std::uint64_t count{0};
+    int nullRefused{0};
+    try { host.CompleteOldestBatchInto(nullptr, 0, output, count); } catch (const std::invalid_argument&) { ++nullRefused; }
     const bool small{host.CompleteOldestBatchInto(buffer.data(), 8, output, count)};
     const bool filled{host.CompleteOldestBatchInto(buffer.data(), buffer.size(), output, count)};
-    std::printf("into %d %d %llu %zu %zu %u %u %llu queries %d\n", small, filled,
+    std::printf("into %d %d %d %llu %zu %zu %u %u %llu queries %d\n", nullRefused, small, filled,
                 static_cast<unsigned long long>(count), output.detections.size(), output.eventStatistics.size(),
                 buffer[11].photon_id, output.eventStatistics[3].event_id,
                 static_cast<unsigned long long>(output.statistics.detected_count), gHandle.queries);
@@ -104,7 +106,8 @@ def test_completion_paths_of_the_cpp_drop_in(tmp_path):
     subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Werror", "-Wno-missing-field-initializers",
                     "-I", str(build.PACKAGE.parent / "include"), str(source), "-o", str(exe)], check=True)
     lines = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines()
-    # refused at capacity 8, then 12 records in the caller's buffer, 4 events, no count query
-    assert lines[0] == "into 0 1 12 0 4 111 21 12 queries 0"
+    # a null buffer refused with the batch still pending, refused at capacity 8, then 12 records
+    # in the caller's buffer, 4 events, no count query
+    assert lines[0] == "into 1 0 1 12 0 4 111 21 12 queries 0"
     # nothing pending: a logic error; CompleteOldestBatch queries once and sizes its vector
     assert lines[1] == "whole 12 4 100 queries 1 refused 1"
