@@ -327,7 +327,9 @@ class GradientRequest(C.Structure):
         ("rindex_material_id", C.c_uint32),
         ("abs_length_material_id", C.c_uint32),
         ("reflectivity_surface_id", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("edge_band_mm", C.c_float),
+        ("edge_index_window", C.c_float),
+        ("reserved", C.c_uint32 * 3),
     ]
 
 

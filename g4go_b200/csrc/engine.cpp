@@ -256,6 +256,11 @@ int Form(const g4b_handle& h) { return h.config.launch_form == G4B_FORM_PLAIN ? 
 // is bound by its tail, so the pass only adds latency there. Config 3 takes
 // the pass for a batch of any size (the same kernels as a large batch's).
 constexpr std::uint64_t kGenerationPassMinPhotons{1ULL << 24};
+// Blocks of a wave's launch over its parked photons.
+constexpr unsigned kParkedBlocks{16U};
+// Default half width of the window in which the gradient replay estimates the
+// boundary term of box edges (edge_band_mm == 0).
+constexpr float kDefaultEdgeBandMm{0.1F};
 bool UsesGenerationPass(const g4b_handle& h) {
     if (Form(h) != g4b::kBatched || Precision(h) != g4b::kFP32 || h.photonCount == 0U) {
         return false;
@@ -915,18 +920,22 @@ std::uint64_t LaunchBatchedWaves(g4b_handle& h, const LaunchParams& base, unsign
               "transport launch");
         Check(cudaEventRecord(h.storeFreeEvent[slot], stream), "cudaEventRecord");
         // the photons the wave parked (they left their volume, or their
-        // history grew long), transported by a second launch of the same
-        // kernel from the queue, with small queue grabs; the wave's ordering
-        // waits for it
+        // history grew long), transported by the kernel's parked-photon form
+        // from the queue, with small queue grabs; the wave's ordering waits
+        // for it. A few blocks: the queue holds little work, but its
+        // longest histories (thousands of steps) keep their blocks resident
+        // long after the rest, and every block slot they hold is one the next
+        // wave's transport cannot use meanwhile.
+        const unsigned parkedGrid{std::min(grid, kParkedBlocks)};
         LaunchParams parked{p};
-        parked.deferred.input = 1U;
         parked.photonBegin = 0U;
         parked.photonEnd = 0U;
         parked.chunk = 32U;
         parked.workTicket = h.dTickets.As<unsigned int>() + kWaveSlots + slot;
         Check(cudaMemsetAsync(parked.workTicket, 0, sizeof(unsigned int), stream), "reset work ticket");
-        Check(g4b::LaunchTransport(parked, g4b::kFP32, KernelOf(h, g4b::kBatched) | g4b::kPregenerated, grid, block,
-                                   SharedBytes(h, g4b::kBatched, block), stream),
+        Check(g4b::LaunchTransport(parked, g4b::kFP32,
+                                   KernelOf(h, g4b::kBatched) | g4b::kPregenerated | g4b::kParkedQueue, parkedGrid,
+                                   block, SharedBytes(h, g4b::kBatched, block), stream),
               "parked photons launch");
         launches += 2;
         if (k + 1U < waves) {
@@ -2045,6 +2054,9 @@ int g4b_gradients(g4b_handle* h, const g4b_gradient_request* request, g4b_gradie
         if (request->abs_length_material_id != kInvalidID && request->abs_length_material_id >= h->materialCount) {
             Throw(G4B_ERR_INVALID_ARGUMENT, "gradient request names an unknown material");
         }
+        if (!std::isfinite(request->edge_band_mm) || !std::isfinite(request->edge_index_window)) {
+            Throw(G4B_ERR_INVALID_ARGUMENT, "gradient request's edge window is not finite");
+        }
         Check(cudaSetDevice(h->device), "cudaSetDevice");
         const std::uint64_t hits{std::min<std::uint64_t>(h->hRun.As<RunCounters>()->hitCount, h->hitCapacity)};
         h->dGradient.Ensure(sizeof(g4b::GradientSums), "cudaMalloc gradient sums");
@@ -2053,8 +2065,12 @@ int g4b_gradients(g4b_handle* h, const g4b_gradient_request* request, g4b_gradie
         Check(cudaEventRecord(h->kernelTimer.start, h->stream), "cudaEventRecord");
         // a grid-stride replay: a few resident 128-thread blocks per SM
         const unsigned grid{static_cast<unsigned>(h->smCount) * 8U};
+        const float band{request->edge_band_mm == 0.0F ? kDefaultEdgeBandMm
+                                                        : (request->edge_band_mm > 0.0F ? request->edge_band_mm : 0.0F)};
+        const float indexWindow{request->edge_index_window > 0.0F ? request->edge_index_window : 0.0F};
         Check(g4b::LaunchGradientReplay(p, Precision(*h), request->rindex_material_id, request->abs_length_material_id,
-                                        request->reflectivity_surface_id, grid, SceneSharedBytes(*h),
+                                        request->reflectivity_surface_id, band, indexWindow, grid,
+                                        SceneSharedBytes(*h),
                                         h->dGradient.As<g4b::GradientSums>(), h->stream),
               "gradient replay");
         Check(cudaEventRecord(h->kernelTimer.stop, h->stream), "cudaEventRecord");

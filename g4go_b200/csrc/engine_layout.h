@@ -188,8 +188,9 @@ constexpr std::uint32_t kPhotonStoreBytes{10U * 4U + 8U + 4U * 4U};  // per phot
 constexpr std::uint32_t kPhotonStoreWave{1U << 26};                  // most photons in one generation wave
 constexpr std::uint32_t kWaveSlots{4};                                // generation-pass waves in flight at once
 
-// A photon of the generation pass's transport parked for the wave's
-// FinishDeferred kernel: the state StepPhoton continues from. Parked are the
+// A photon of the generation pass's transport parked in the wave's queue,
+// which the parked-photon form of the pass kernel transports: the state
+// StepPhoton continues from. Parked are the
 // photons that leave their volume the way the reference lets them (a trace
 // that has to search the whole scene; some then reflect totally at every step
 // for thousands of steps) and any history that reaches kDeferBounces bounces.
@@ -215,7 +216,7 @@ struct DeferredQueue {
     DeferredPhoton* photons;  // nullptr: no deferral
     unsigned int* count;      // photons parked; may exceed capacity (those beyond stay in their lane)
     std::uint32_t capacity;
-    std::uint32_t input;      // 1: the launch transports the parked photons instead of the store's
+    std::uint32_t reserved;
 };
 constexpr std::uint32_t kDeferBounces{256};
 constexpr std::uint32_t kDeferredCapacity{1U << 19};  // per wave in flight (38 MB each)

@@ -11,13 +11,14 @@
 namespace g4b {
 
 enum KernelPrecision : int { kFP32 = 0, kFP64 = 1 };
-enum KernelForm : int { kBatched = 0, kPlain = 1, kWithDiagnostics = 2, kPregenerated = 4 };
+enum KernelForm : int { kBatched = 0, kPlain = 1, kWithDiagnostics = 2, kPregenerated = 4, kParkedQueue = 8 };
 
 // The transport kernel for (precision, form), as a function pointer usable in
 // cudaLaunchKernel and in graph kernel nodes. `form` may carry
 // kWithDiagnostics (the variant that also counts coincident-face retraces)
 // and, for the batched FP32 form, kPregenerated (photons read from the
-// photon store instead of generated in the loop).
+// photon store instead of generated in the loop), with kParkedQueue too
+// (photons read from the wave's queue of parked photons).
 const void* TransportKernel(int precision, int form);
 const void* GenerateKernel();
 const void* ZeroCountersKernel();
@@ -77,11 +78,14 @@ cudaError_t LaunchOrderRecordsStatic(const void* records, const std::uint32_t* k
 
 // Gradient replay over the photons [photonBegin, photonEnd) of the last
 // transport: each one is regenerated and re-transported from its RNG counters
-// with dual numbers, alternate branches of its Fresnel choices transported
-// when an index target is set, and its derivative terms summed into `sums`.
+// with dual numbers, alternate branches of its Fresnel choices and of its
+// exits near box edges (within edgeBand mm, or the distance a fast edge moves
+// over +-edgeIndexWindow in n; edgeBand 0: no edge term) transported when an
+// index target is set, and its derivative terms summed into `sums`.
 cudaError_t LaunchGradientReplay(const LaunchParams& params, int precision, std::uint32_t indexMaterial,
-                                 std::uint32_t absMaterial, std::uint32_t reflectivitySurface, unsigned grid,
-                                 std::size_t sharedBytes, GradientSums* sums, cudaStream_t stream);
+                                 std::uint32_t absMaterial, std::uint32_t reflectivitySurface, float edgeBand,
+                                 float edgeIndexWindow, unsigned grid, std::size_t sharedBytes, GradientSums* sums,
+                                 cudaStream_t stream);
 
 cudaError_t LaunchEvalFresnel(int precision, std::uint32_t n, const double* in, double* out, cudaStream_t stream);
 cudaError_t LaunchEvalLambertian(int precision, std::uint32_t n, const double* in, double* out, cudaStream_t stream);

@@ -223,8 +223,9 @@ __device__ __forceinline__ bool LoadStoredPhoton(const PhotonStore& store, std::
     return true;
 }
 
-// Parks a photon whose history reached kDeferBounces in the wave's queue for
-// FinishDeferred; false (the photon stays in its lane) when the queue is full.
+// Parks a photon (it left its volume, or its history reached kDeferBounces)
+// in the wave's queue, which a second launch of the pass kernel transports;
+// false (the photon stays in its lane) when the queue is full.
 __device__ __forceinline__ bool DeferPhoton(const DeferredQueue& queue, const Photon<float>& photon) {
     const unsigned int i{atomicAdd(queue.count, 1U)};
     if (i >= queue.capacity) {
@@ -488,7 +489,12 @@ struct BatchedMinBlocks<double> {
 // without it the counting is compiled out, which frees registers in the loop.
 // kPregenerated (FP32 only): the wave's photons come from the photon store
 // that GeneratePhotons filled, and the loop carries no generation code.
-template<class R, bool kDiagnostics, bool kPregenerated = false>
+// kParked (with kPregenerated): the photons come from the wave's queue of
+// parked photons instead, and each step completes its Fresnel boundary in
+// place: what the queue holds is few photons with long histories, whose
+// steps should each take one loop iteration, not the three that parking in
+// the ring costs a lone photon.
+template<class R, bool kDiagnostics, bool kPregenerated = false, bool kParked = false>
 __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatched(const LaunchParams p) {
     LoadScene(p);
     const PackedScene& scene{*reinterpret_cast<const PackedScene*>(gShared)};
@@ -496,11 +502,12 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
     const unsigned lane{threadIdx.x & 31U};
     const unsigned lanesBelow{(1U << lane) - 1U};
     const R epsilon{R(p.epsilon)};
-    // the pass form's second launch per wave takes the photons the first one
-    // parked, and parks none itself
-    const bool fromQueue{kPregenerated && p.deferred.input != 0U};
-    const std::uint32_t totalPhotons{fromQueue ? min(*p.deferred.count, p.deferred.capacity)
-                                               : p.photonEnd - p.photonBegin};
+    static_assert(!kParked || kPregenerated, "the parked-photon form reads the pass form's queue");
+    // whether this lane may still park photons in the wave's queue (the
+    // parked form parks none itself)
+    bool parkOpen{kPregenerated && !kParked && p.deferred.photons != nullptr};
+    const std::uint32_t totalPhotons{kParked ? min(*p.deferred.count, p.deferred.capacity)
+                                             : p.photonEnd - p.photonBegin};
     const std::uint32_t sceneEnd{(p.sceneBytes + 15U) & ~15U};
     // shared memory: scene, then one photon queue per warp (not with
     // kPregenerated: lanes take photons straight from the store), one Fresnel
@@ -587,7 +594,7 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
                 const std::uint32_t rank{static_cast<std::uint32_t>(__popc(need & lanesBelow))};
                 if (((need >> lane) & 1U) != 0U && rank < available) {
                     const std::uint32_t slot{chunkNext + rank};
-                    if (fromQueue) {
+                    if constexpr (kParked) {
                         LoadDeferredPhoton(p.deferred, slot - p.photonBegin, photon);
                         counters.Switch(photon.eventIndex, p.events);
                         alive = true;
@@ -685,28 +692,25 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
         std::uint32_t result{kContinue};
         StepExtras extras{0U, 0U, 0U, 0U};
         FresnelJob<R> job;
-        // the pass form hands photons that leave their volume to the wave's
-        // FinishDeferred kernel while its queue has room (read once per warp
-        // iteration; a stale read only delays a hand-over by one step)
-        bool deferLeft{false};
-        if constexpr (kPregenerated) {
-            unsigned int parked{0U};
-            if (lane == 0U && p.deferred.photons != nullptr && !fromQueue) {
-                parked = *reinterpret_cast<volatile unsigned int*>(p.deferred.count);
-            }
-            parked = __shfl_sync(kFullMask, parked, 0);
-            deferLeft = p.deferred.photons != nullptr && !fromQueue && parked < p.deferred.capacity;
-        }
         if (alive) {
-            result = StepPhoton<R, true>(scene, pool, photon, p.seed, p.maxBounce, epsilon, extras, NoGradient(), &job,
-                                         deferLeft);
+            if constexpr (kParked) {
+                result = StepPhoton<R>(scene, pool, photon, p.seed, p.maxBounce, epsilon, extras, NoGradient());
+            } else {
+                // the pass form parks photons that leave their volume in the
+                // wave's queue, for the queue's own launch, until the lane
+                // finds the queue full
+                result = StepPhoton<R, true>(scene, pool, photon, p.seed, p.maxBounce, epsilon, extras, NoGradient(),
+                                             &job, parkOpen);
+            }
         }
         if constexpr (kPregenerated) {
             if (alive && result == kLeftVolume) {
                 // untouched by the step: handed over whole, or (queue full)
-                // stepped again next iteration with deferLeft false
+                // stepped again next iteration, now in place
                 if (DeferPhoton(p.deferred, photon)) {
                     alive = false;
+                } else {
+                    parkOpen = false;
                 }
                 result = kContinue;
             }
@@ -758,11 +762,14 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
             }
         }
         if constexpr (kPregenerated) {
-            // a long history goes to the wave's FinishDeferred kernel, and the
-            // lane takes fresh work (identical results: the step is the same)
-            if (alive && photon.bounce >= kDeferBounces && p.deferred.photons != nullptr && !fromQueue &&
-                DeferPhoton(p.deferred, photon)) {
-                alive = false;
+            // a long history goes to the wave's queue launch, and the lane
+            // takes fresh work (identical results: the step is the same)
+            if (alive && photon.bounce >= kDeferBounces && parkOpen) {
+                if (DeferPhoton(p.deferred, photon)) {
+                    alive = false;
+                } else {
+                    parkOpen = false;
+                }
             }
         }
         __syncwarp();
@@ -843,6 +850,24 @@ __device__ __forceinline__ unsigned long long AlternateSeed(unsigned long long s
     return seed ^ (0x9E3779B97F4A7C15ULL * (static_cast<unsigned long long>(bounce) + 1ULL));
 }
 
+// Transports `branch` to its end with the draws of `seed`. Returns whether it
+// was detected and its arrival time.
+template<class R>
+__device__ bool RunBranch(const PackedScene& scene, const float* pool, const LaunchParams& p, Photon<R>& branch,
+                          unsigned long long seed, double* time) {
+    if (branch.bounce >= p.maxBounce) {
+        return false;
+    }
+    const R epsilon{R(p.epsilon)};
+    StepExtras extras{0U, 0U, 0U, 0U};
+    std::uint32_t result;
+    do {
+        result = StepPhoton<R>(scene, pool, branch, seed, p.maxBounce, epsilon, extras, NoGradient());
+    } while (result == kContinue);
+    *time = branch.time;
+    return result == kDetected;
+}
+
 // Transports the branch a replayed photon did not take at its last Fresnel
 // choice to its end in plain arithmetic. Returns whether it was detected and
 // its arrival time.
@@ -859,31 +884,41 @@ __device__ bool RunAlternate(const PackedScene& scene, const float* pool, const 
     branch.bounce = taken.bounce;
     branch.eventID = taken.eventID;
     branch.photonID = taken.photonID;
-    if (branch.bounce >= p.maxBounce) {
-        return false;
-    }
-    const unsigned long long seed{AlternateSeed(p.seed, taken.bounce)};
-    const R epsilon{R(p.epsilon)};
-    StepExtras extras{0U, 0U, 0U, 0U};
-    std::uint32_t result;
-    do {
-        result = StepPhoton<R>(scene, pool, branch, seed, p.maxBounce, epsilon, extras, NoGradient());
-    } while (result == kContinue);
-    *time = branch.time;
-    return result == kDetected;
+    return RunBranch(scene, pool, p, branch, AlternateSeed(p.seed, taken.bounce), time);
+}
+
+// Transports the state a replayed photon's last step left for its edge term
+// (the same step, its ray leaving through the face beyond the edge) to its
+// end in plain arithmetic, with the photon's own draws.
+template<class R>
+__device__ bool RunEdgeBranch(const PackedScene& scene, const float* pool, const LaunchParams& p,
+                              const Photon<Dual<R>>& taken, double* time) {
+    Photon<R> branch{};
+    branch.position = taken.tangents.edgePosition;
+    branch.direction = taken.tangents.edgeDirection;
+    branch.polarization = taken.tangents.edgePolarization;
+    branch.volume = taken.tangents.edgeVolume;
+    branch.time = taken.tangents.edgeTime;
+    branch.energy = taken.energy.v;
+    branch.bounce = taken.tangents.edgeBounce;
+    branch.eventID = taken.eventID;
+    branch.photonID = taken.photonID;
+    return RunBranch(scene, pool, p, branch, p.seed, time);
 }
 
 // Gradient replay: every photon of the batch is regenerated from its RNG
 // counters and re-transported with dual numbers (pathwise derivatives), its
 // score terms accumulating; with a refractive-index target each Fresnel choice
 // at a boundary without a surface spawns its alternate branch instead of a
-// score (measure-valued derivative, bounded where the score dT/T is not).
+// score (measure-valued derivative, bounded where the score dT/T is not),
+// and each step that leaves its box near an edge the branch through the face
+// beyond it (SpawnEdgeBranch: the boundary term of the moving edge).
 // Per photon, with f its detection and t its arrival time:
 //   dN     += f (S + W) - sum_k w_k f_k
 //   d(tN)  += f (t (S + W) + dt) - sum_k w_k f_k t_k
-// where S is the score, w_k = +-dT/dn of choice k, W = sum w_k and f_k, t_k the
-// outcome of its alternate. Grid-stride over the photons, FP64 sums reduced
-// per warp at the end.
+// where S is the score, w_k = +-dT/dn of Fresnel choice k or the weight of
+// edge term k, W = sum w_k and f_k, t_k the outcome of its branch.
+// Grid-stride over the photons, FP64 sums reduced per warp at the end.
 template<class R>
 __global__ void __launch_bounds__(128) GradientReplay(const LaunchParams p, GradientTargets targets,
                                                       GradientSums* sums) {
@@ -917,6 +952,16 @@ __global__ void __launch_bounds__(128) GradientReplay(const LaunchParams p, Grad
                     double time{0.0};
                     weights += w;
                     if (RunAlternate(scene, pool, p, photon, &time)) {
+                        alternateDetected += w;
+                        alternateTime += w * time;
+                    }
+                }
+                if (photon.tangents.edgePending) {
+                    photon.tangents.edgePending = false;
+                    const double w{photon.tangents.edgeWeight};
+                    double time{0.0};
+                    weights += w;
+                    if (RunEdgeBranch(scene, pool, p, photon, &time)) {
                         alternateDetected += w;
                         alternateTime += w * time;
                     }
@@ -1318,6 +1363,10 @@ const void* TransportKernel(int precision, int form) {
         return diagnostics ? reinterpret_cast<const void*>(&TransportBatched<double, true>)
                            : reinterpret_cast<const void*>(&TransportBatched<double, false>);
     }
+    if ((form & kParkedQueue) != 0) {
+        return diagnostics ? reinterpret_cast<const void*>(&TransportBatched<float, true, true, true>)
+                           : reinterpret_cast<const void*>(&TransportBatched<float, false, true, true>);
+    }
     if ((form & kPregenerated) != 0) {
         return diagnostics ? reinterpret_cast<const void*>(&TransportBatched<float, true, true>)
                            : reinterpret_cast<const void*>(&TransportBatched<float, false, true>);
@@ -1333,8 +1382,8 @@ const void* ZeroCountersKernel() { return reinterpret_cast<const void*>(&ZeroCou
 cudaError_t ConfigureTransportKernels(std::size_t sharedBytes) {
     for (int precision = 0; precision < 2; ++precision) {
         // kBatched, kPlain, each with and without kWithDiagnostics, and the
-        // pregenerated batched kernels (FP32)
-        constexpr int kForms[]{0, 1, 2, 3, 4, 6};
+        // pregenerated and parked-photon batched kernels (FP32)
+        constexpr int kForms[]{0, 1, 2, 3, 4, 6, 12, 14};
         for (const int form : kForms) {
             const cudaError_t error{cudaFuncSetAttribute(TransportKernel(precision, form),
                                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1458,9 +1507,10 @@ cudaError_t LaunchOrderRecordsStatic(const void* records, const std::uint32_t* k
 }
 
 cudaError_t LaunchGradientReplay(const LaunchParams& params, int precision, std::uint32_t indexMaterial,
-                                 std::uint32_t absMaterial, std::uint32_t reflectivitySurface, unsigned grid,
-                                 std::size_t sharedBytes, GradientSums* sums, cudaStream_t stream) {
-    const GradientTargets targets{indexMaterial, absMaterial, reflectivitySurface};
+                                 std::uint32_t absMaterial, std::uint32_t reflectivitySurface, float edgeBand,
+                                 float edgeIndexWindow, unsigned grid, std::size_t sharedBytes, GradientSums* sums,
+                                 cudaStream_t stream) {
+    const GradientTargets targets{indexMaterial, absMaterial, reflectivitySurface, edgeBand, edgeIndexWindow};
     const void* kernel{precision == kFP64 ? reinterpret_cast<const void*>(&GradientReplay<double>)
                                           : reinterpret_cast<const void*>(&GradientReplay<float>)};
     cudaError_t error{cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

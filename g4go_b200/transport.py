@@ -570,9 +570,18 @@ class TransportHost:
     PARAMETERS = ("rindex", "abs_length_mm", "reflectivity", "decay_time_ns")
 
     def gradients(self, rindex_material: int = INVALID_ID, abs_length_material: int = INVALID_ID,
-                  reflectivity_surface: int = INVALID_ID) -> dict:
-        """d(detected)/d theta and d(mean arrival time)/d theta for the last completed batch."""
-        request = _abi.GradientRequest(rindex_material, abs_length_material, reflectivity_surface, 0)
+                  reflectivity_surface: int = INVALID_ID, edge_band_mm: float | None = None,
+                  edge_index_window: float | None = None) -> dict:
+        """d(detected)/d theta and d(mean arrival time)/d theta for the last completed batch.
+
+        The index derivative's boundary term of box edges is estimated in a
+        window of half width edge_band_mm (None: the library's 0.1 mm; 0: no
+        boundary term), widened for fast edges to the distance they move over
+        +-edge_index_window in n when that is given (lower variance, a bias
+        growing with it)."""
+        band = 0.0 if edge_band_mm is None else (float(edge_band_mm) if edge_band_mm > 0 else -1.0)
+        window = float(edge_index_window) if edge_index_window else 0.0
+        request = _abi.GradientRequest(rindex_material, abs_length_material, reflectivity_surface, band, window)
         result = _abi.Gradients()
         self._check(self._lib.g4b_gradients(self._handle, C.byref(request), C.byref(result)))
         return {

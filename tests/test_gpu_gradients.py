@@ -17,14 +17,16 @@ resolves nothing there: they use steps of 1e-2 and must lie within four
 standard errors. The decay-time derivative of the mean time is large and is
 held to 2 %.
 
-The refractive-index derivative omits geometric boundary terms: when a
+The refractive-index derivative also has a geometric boundary term: when a
 change of n moves a refracted ray across the edge of a face, the photon's
 fate changes discontinuously, and neither a pathwise nor a score term sees
 that. Near the critical angle the rays refracted into the 0.1 mm grease run
 almost parallel to it and travel far sideways, so the edges of the coupling
-layer matter: with the standard 3x3 mm layer the edge term is about half of
-dN/dn, with a 40 mm layer about 3 %. dN/dn is therefore checked on a 1 m
-coupling layer, where grazing rays reach the SiPM before any edge.
+layer matter: with the standard 3x3 mm layer that term is about half of
+dN/dn. The replay estimates it at every step that leaves its box close to an
+edge (g4b_gradient_request.edge_band_mm). dN/dn is checked on the standard
+detector at three indices, and on a 1 m coupling layer, where grazing rays
+reach the SiPM before any edge, as unit cases of the other terms.
 """
 import numpy as np
 import pytest
@@ -163,3 +165,49 @@ def test_index_gradient_with_a_reflective_wrapper(base_batch):
     dn, dn_se, _, _ = central_differences(theta0, base_batch, 1000.0, 0)
     print(f"\ndN/dn replay {grad_detected[0]:.6g} FD {dn:.6g} +- {dn_se:.3g} ratio {grad_detected[0] / dn:.4f}")
     assert agrees(grad_detected[0], dn, dn_se), (grad_detected[0], dn, dn_se)
+
+
+STANDARD_EVENTS = 24000  # 1.2e9 photons: the replay's standard error stays below 1 %
+INDEX_STEP = 3e-3  # relative; central differences with 1e-3 agree within their errors
+
+
+def event_parts(batch, parts):
+    """The batch's events dealt into `parts` batches (event i into part i mod parts)."""
+    events = np.arange(batch.event_ids.shape[0])
+    out = []
+    for part in range(parts):
+        chosen = events[events % parts == part]
+        keep = np.isin(batch.emission_event_indices, chosen)
+        index = np.full(events.shape[0], -1, np.int64)
+        index[chosen] = np.arange(chosen.shape[0])
+        out.append(PhotonTransportBatch(batch.emissions[keep], batch.event_ids[chosen],
+                                        index[batch.emission_event_indices[keep]].astype(np.uint32)))
+    return out
+
+
+@pytest.mark.parametrize("n", [1.70, 1.82, 1.90])
+def test_index_gradient_on_the_standard_detector(n):
+    """dN/dn on the benchmark's detector (3x3 mm coupling layer, reflective
+    wrapper) with the boundary term of the layer's edges, against central
+    differences with common random numbers, within 2 %. Both standard errors
+    come from the spread over GROUPS parts of the events (the replay is run
+    part by part, the finite difference counted part by part); together they
+    must stay below 1 % so that 2 % is resolved."""
+    base = scenes.workload("gradients", event_count=STANDARD_EVENTS, seed=5)
+    scene = scenes.crystal_sipm_scene(scenes.DetectorParameters(crystal_rindex=n))
+    replay = []
+    with TransportHost(PhotonTransportConfig(seed=SEED, precision="fp32")) as host:
+        for part in event_parts(base, GROUPS):
+            host.enqueue_emissions(scene, part)
+            host.complete_oldest_batch()
+            grads = host.gradients(scenes.MAT_CRYSTAL)
+            assert grads["replay_mismatches"] == 0
+            replay.append(grads["d_detected"]["rindex"])
+    replay = np.array(replay)
+    dn, replay_se = replay.sum(), replay.std(ddof=1) * np.sqrt(GROUPS)
+    fd, fd_se, _, _ = central_differences((n, 400.0, 0.95, 40.0), base, None, 0, INDEX_STEP)
+    combined = np.hypot(replay_se, fd_se)
+    print(f"\nn={n}: dN/dn replay {dn:.6g} +- {replay_se:.3g}, FD {fd:.6g} +- {fd_se:.3g}; "
+          f"difference {(dn - fd) / fd:+.2%}, standard error of the difference {combined / abs(fd):.2%}")
+    assert combined < 0.01 * abs(fd), (dn, replay_se, fd, fd_se)
+    assert abs(dn - fd) <= 0.02 * abs(fd), (dn, replay_se, fd, fd_se)
