@@ -173,21 +173,29 @@ struct g4b_handle {
     std::uint64_t hitCapacity{0};
     DeviceBuffer dBitmap, dPrefix, dBlockSums, dDetections, dFate, dFateTime, dGradient;
     // kWaveSlots photon stores and work tickets of the generation pass: wave k
-    // uses slot k % kWaveSlots, and its transport runs on transport stream
-    // k % kWaveSlots (the handle's stream, then waveStreams). Up to kWaveSlots
-    // waves are in flight, so a wave's longest photon histories - serial
-    // chains of thousands of steps - overlap the next waves' transports
-    // instead of holding up the GPU.
+    // uses slot k % kWaveSlots, and its transport and parked-photon launch run
+    // on transport stream k % kWaveSlots (the handle's stream, then
+    // waveStreams). Up to kWaveSlots waves are in flight, so a wave's longest
+    // photon histories - serial chains of thousands of steps - overlap the
+    // next waves' transports instead of holding up the GPU. The waves' hit
+    // orderings and row copies run in wave order on orderStream, so that a
+    // transport stream never waits for an ordering: those kernels get SMs
+    // only when a transport's blocks leave, and a transport queued behind one
+    // would start only after the previous wave's transport had drained.
     DeviceBuffer dStore;
     DeviceBuffer dTickets;
-    DeviceBuffer dDeferred;        // per slot: kDeferredCapacity parked long histories
+    DeviceBuffer dDeferred;        // per slot: deferredCapacity parked photons
+    std::uint32_t deferredCapacity{0};
+    std::uint64_t waveLimit{0};    // most photons per wave for the staged batch (set by SizeWaves)
     DeviceBuffer dDeferredCounts;  // per slot: how many were parked
     cudaStream_t generationStream{nullptr};
     cudaStream_t waveStreams[kWaveSlots - 1]{};
     cudaEvent_t zeroedEvent{nullptr};
     cudaEvent_t generatedEvent[kWaveSlots]{};
     cudaEvent_t storeFreeEvent[kWaveSlots]{};
-    cudaEvent_t orderedEvent[2]{};  // a wave's ordering done (the next wave's ordering follows it)
+    cudaEvent_t parkedEvent[kWaveSlots]{};  // a wave's parked photons transported: its hits can be ordered
+    cudaStream_t orderStream{nullptr};
+    cudaEvent_t orderJoinEvent{nullptr};  // the ordering stream's last work, joined into the handle's stream
     cudaEvent_t joinEvents[kWaveSlots - 1]{};  // each wave stream's last work, joined into the handle's stream
     cudaGraphExec_t wavesExec{nullptr};  // the generation-pass waves of the last batch, captured
     // Per-wave hits and ordering of the generation-pass form: wave k writes its
@@ -749,15 +757,15 @@ void LaunchBatchedGraph(g4b_handle& h, const LaunchParams& params, unsigned grid
 }
 
 // Photons per wave of the generation pass: the batch cut into equal waves
-// of at most kPhotonStoreWave, or of at most the configured wave_photons.
-std::uint64_t WavePhotons(const g4b_handle& h) {
-    const std::uint64_t limit{h.config.wave_photons != 0U
-                                  ? std::min<std::uint64_t>((h.config.wave_photons + 31ULL) / 32ULL * 32ULL,
-                                                            g4b::kPhotonStoreWave)
-                                  : g4b::kPhotonStoreWave};
-    const std::uint64_t waves{(h.photonCount + limit - 1U) / limit};
+// of at most `limit` photons.
+std::uint64_t EqualWaves(std::uint64_t photons, std::uint64_t limit) {
+    const std::uint64_t waves{(photons + limit - 1U) / limit};
     // a multiple of 32, so every wave starts on a word of the slot bitmap
-    return waves == 0U ? 0U : ((h.photonCount + waves - 1U) / waves + 31U) / 32U * 32U;
+    return waves == 0U ? 0U : ((photons + waves - 1U) / waves + 31U) / 32U * 32U;
+}
+
+std::uint64_t WavePhotons(const g4b_handle& h) {
+    return EqualWaves(h.photonCount, h.waveLimit != 0U ? h.waveLimit : g4b::kPhotonStoreWaveMin);
 }
 
 // Bytes of one photon store for `rows` photons: 256-byte aligned columns.
@@ -765,6 +773,37 @@ std::size_t StoreBytes(std::uint64_t rows) {
     const auto rounded{[](std::size_t bytes) { return (bytes + 255U) & ~std::size_t{255}; }};
     return 10U * rounded(rows * sizeof(float)) + rounded(rows * sizeof(double)) +
            4U * rounded(rows * sizeof(std::uint32_t));
+}
+
+// Wave size of the staged batch. The configured wave_photons, else the
+// largest limit from kPhotonStoreWave down to kPhotonStoreWaveMin (halving)
+// whose stores - one per wave in flight - fit in half of the device memory
+// that is free or already held by this handle's stores: fewer, larger waves
+// pay fewer wave changes (each a transport's drain and a generation not
+// hidden behind it), and the stores of the benchmark's 1.1e9-photon batch
+// take 58 GB at 2^28 photons per wave. The parked-photon queues hold 1/64 of
+// a wave each, at least kDeferredMinCapacity.
+void SizeWaves(g4b_handle& h) {
+    if (h.config.wave_photons != 0U) {
+        h.waveLimit = std::min<std::uint64_t>((h.config.wave_photons + 31ULL) / 32ULL * 32ULL, g4b::kPhotonStoreWave);
+    } else {
+        std::size_t free{0};
+        std::size_t total{0};
+        Check(cudaMemGetInfo(&free, &total), "cudaMemGetInfo");
+        const std::size_t budget{(free + h.dStore.bytes) / 2U};
+        std::uint64_t limit{g4b::kPhotonStoreWave};
+        while (limit > g4b::kPhotonStoreWaveMin) {
+            const std::uint64_t wave{EqualWaves(h.photonCount, limit)};
+            const std::uint64_t waves{wave == 0U ? 0U : (h.photonCount + wave - 1U) / wave};
+            if (std::min<std::uint64_t>(waves, kWaveSlots) * StoreBytes(wave) <= budget) {
+                break;
+            }
+            limit /= 2U;
+        }
+        h.waveLimit = limit;
+    }
+    h.deferredCapacity = static_cast<std::uint32_t>(
+        std::max<std::uint64_t>(g4b::kDeferredMinCapacity, WavePhotons(h) / 64U));
 }
 
 // Column views of photon store `which` (0 or 1) of the handle's allocation,
@@ -809,29 +848,33 @@ void EnsureGenerationStream(g4b_handle& h) {
         Check(cudaStreamCreateWithFlags(&h.waveStreams[k], cudaStreamNonBlocking), "cudaStreamCreateWithFlags");
         Check(cudaEventCreateWithFlags(&h.joinEvents[k], cudaEventDisableTiming), "cudaEventCreate");
     }
-    for (auto& event : h.orderedEvent) {
+    for (auto& event : h.parkedEvent) {
         Check(cudaEventCreateWithFlags(&event, cudaEventDisableTiming), "cudaEventCreate");
     }
+    Check(cudaStreamCreateWithFlags(&h.orderStream, cudaStreamNonBlocking), "cudaStreamCreateWithFlags");
+    Check(cudaEventCreateWithFlags(&h.orderJoinEvent, cudaEventDisableTiming), "cudaEventCreate");
 }
 
 // Batched FP32 form with a generation pass. The batch is cut into equal waves
 // of at most kPhotonStoreWave photons. GeneratePhotons fills a wave's store
 // on the generation stream, and the transport kernel then takes the wave's
-// photons from it. The two stores and work tickets alternate, so wave k+1 is
-// generated while wave k is transported: its blocks fill the SMs that wave
-// k's finished warps leave. The transports alternate between two streams as
-// well, so wave k+1's transport also starts while wave k's last warps still
-// run their longest photon histories; each wave has its own region of the hit
-// buffer and its own row counter for that. The waves' orderings run in wave
-// order. Counters are zeroed once per batch. Returns the number of kernels
-// launched.
+// photons from it. Up to kWaveSlots stores and work tickets rotate, so wave
+// k+1 is generated while wave k is transported: its blocks fill the SMs that
+// wave k's finished warps leave. The transports rotate over kWaveSlots
+// streams as well, so wave k+1's transport also starts while wave k's last
+// warps still run their longest photon histories; each wave has its own
+// region of the hit buffer and its own row counter for that. A wave's parked
+// photons follow its transport on its stream. The waves' orderings run in
+// wave order on a stream of their own. Counters are zeroed once per batch.
+// LaunchBatchedWaves returns the number of kernels launched.
 void PrepareWaves(g4b_handle& h) {
     EnsureGenerationStream(h);
     const std::uint64_t wave{WavePhotons(h)};
     const std::uint64_t waves{(h.photonCount + wave - 1U) / wave};
-    h.dStore.Ensure(kWaveSlots * StoreBytes(wave), "cudaMalloc photon stores");
+    // a store per wave in flight: fewer for a batch of fewer waves
+    h.dStore.Ensure(std::min<std::uint64_t>(waves, kWaveSlots) * StoreBytes(wave), "cudaMalloc photon stores");
     h.dTickets.Ensure(2U * kWaveSlots * sizeof(unsigned int), "cudaMalloc work tickets");  // waves, parked photons
-    h.dDeferred.Ensure(std::size_t{kWaveSlots} * g4b::kDeferredCapacity * sizeof(g4b::DeferredPhoton),
+    h.dDeferred.Ensure(std::size_t{kWaveSlots} * h.deferredCapacity * sizeof(g4b::DeferredPhoton),
                        "cudaMalloc deferred photons");
     h.dDeferredCounts.Ensure(kWaveSlots * sizeof(unsigned int), "cudaMalloc deferred counts");
     h.dWaveCounts.Ensure(waves * sizeof(unsigned long long), "cudaMalloc wave counts");
@@ -885,9 +928,9 @@ std::uint64_t LaunchBatchedWaves(g4b_handle& h, const LaunchParams& base, unsign
         p.workTicket = h.dTickets.As<unsigned int>() + k % kWaveSlots;
         p.hits = HitRegion(base.hits, k * h.waveRegionRows, h.waveRegionRows);
         p.hitCounter = waveCounts + k;
-        p.deferred.photons = h.dDeferred.As<g4b::DeferredPhoton>() + (k % kWaveSlots) * g4b::kDeferredCapacity;
+        p.deferred.photons = h.dDeferred.As<g4b::DeferredPhoton>() + (k % kWaveSlots) * h.deferredCapacity;
         p.deferred.count = h.dDeferredCounts.As<unsigned int>() + k % kWaveSlots;
-        p.deferred.capacity = g4b::kDeferredCapacity;
+        p.deferred.capacity = h.deferredCapacity;
         return p;
     }};
     cudaStream_t streams[kWaveSlots]{h.stream};
@@ -903,6 +946,7 @@ std::uint64_t LaunchBatchedWaves(g4b_handle& h, const LaunchParams& base, unsign
     for (cudaStream_t stream : h.waveStreams) {
         Check(cudaStreamWaitEvent(stream, h.zeroedEvent, 0), "cudaStreamWaitEvent");
     }
+    Check(cudaStreamWaitEvent(h.orderStream, h.zeroedEvent, 0), "cudaStreamWaitEvent");
     Check(g4b::LaunchGenerate(waveParams(0), generateGrid, SceneSharedBytes(h), h.generationStream),
           "generation launch");
     Check(cudaEventRecord(h.generatedEvent[0], h.generationStream), "cudaEventRecord");
@@ -922,11 +966,11 @@ std::uint64_t LaunchBatchedWaves(g4b_handle& h, const LaunchParams& base, unsign
         // the photons the wave parked (they left their volume, or their
         // history grew long), transported by the kernel's parked-photon form
         // from the queue, with small queue grabs; the wave's ordering waits
-        // for it. A few blocks: the queue holds little work, but its
-        // longest histories (thousands of steps) keep their blocks resident
-        // long after the rest, and every block slot they hold is one the next
-        // wave's transport cannot use meanwhile.
-        const unsigned parkedGrid{std::min(grid, kParkedBlocks)};
+        // for it. A few blocks, but for the last wave: the queue holds little
+        // work, but its longest histories (thousands of steps) keep their
+        // blocks resident long after the rest, and every block slot they hold
+        // is one the next wave's transport cannot use meanwhile.
+        const unsigned parkedGrid{k + 1U == waves ? grid : std::min(grid, kParkedBlocks)};
         LaunchParams parked{p};
         parked.photonBegin = 0U;
         parked.photonEnd = 0U;
@@ -937,6 +981,7 @@ std::uint64_t LaunchBatchedWaves(g4b_handle& h, const LaunchParams& base, unsign
                                    KernelOf(h, g4b::kBatched) | g4b::kPregenerated | g4b::kParkedQueue, parkedGrid,
                                    block, SharedBytes(h, g4b::kBatched, block), stream),
               "parked photons launch");
+        Check(cudaEventRecord(h.parkedEvent[slot], stream), "cudaEventRecord");
         launches += 2;
         if (k + 1U < waves) {
             const std::uint32_t next{static_cast<std::uint32_t>((k + 1U) % kWaveSlots)};
@@ -948,31 +993,31 @@ std::uint64_t LaunchBatchedWaves(g4b_handle& h, const LaunchParams& base, unsign
             Check(cudaEventRecord(h.generatedEvent[next], h.generationStream), "cudaEventRecord");
             ++launches;
         }
-        // order this wave's hits after the previous wave's, while the next
-        // wave is generated and transported
-        if (k >= 1U) {
-            Check(cudaStreamWaitEvent(stream, h.orderedEvent[(k + 1U) % 2U], 0), "cudaStreamWaitEvent");
-        }
+        // order this wave's hits after the previous wave's, on the ordering
+        // stream, while the next waves are generated and transported
+        Check(cudaStreamWaitEvent(h.orderStream, h.parkedEvent[slot], 0), "cudaStreamWaitEvent");
         Check(g4b::LaunchOrderWaveHits(p.hits, waveCounts + k, waveRows + k, base.run, p.photonBegin, p.photonEnd,
                                        h.dBitmap.As<std::uint32_t>(), h.dPrefix.As<std::uint32_t>(),
                                        h.dBlockSums.As<std::uint32_t>(), h.dDetections.pointer, ordered,
-                                       static_cast<unsigned>(h.smCount) * 4U, stream),
+                                       static_cast<unsigned>(h.smCount) * 4U, h.orderStream),
               "wave hit ordering");
         launches += ordered ? 6U : 2U;
-        Check(cudaEventRecord(h.orderedEvent[k % 2U], stream), "cudaEventRecord");
         Check(cudaMemcpyAsync(h.hWaveRows.As<unsigned long long>() + k + 1U, waveRows + k + 1U,
-                              sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream),
+                              sizeof(unsigned long long), cudaMemcpyDeviceToHost, h.orderStream),
               "cudaMemcpyAsync wave rows to host");
         // inside a capture the record must stay a real event record for the host to wait on
-        Check(capturing ? cudaEventRecordWithFlags(h.waveEvents[k], stream, cudaEventRecordExternal)
-                        : cudaEventRecord(h.waveEvents[k], stream),
+        Check(capturing ? cudaEventRecordWithFlags(h.waveEvents[k], h.orderStream, cudaEventRecordExternal)
+                        : cudaEventRecord(h.waveEvents[k], h.orderStream),
               "cudaEventRecord wave");
     }
-    // the other transport streams' last work joins the handle's stream
+    // the other transport streams' and the ordering stream's last work joins
+    // the handle's stream
     for (std::uint32_t k{}; k + 1U < kWaveSlots; ++k) {
         Check(cudaEventRecord(h.joinEvents[k], h.waveStreams[k]), "cudaEventRecord");
         Check(cudaStreamWaitEvent(h.stream, h.joinEvents[k], 0), "cudaStreamWaitEvent");
     }
+    Check(cudaEventRecord(h.orderJoinEvent, h.orderStream), "cudaEventRecord");
+    Check(cudaStreamWaitEvent(h.stream, h.orderJoinEvent, 0), "cudaStreamWaitEvent");
     return launches;
 }
 
@@ -1037,6 +1082,9 @@ void RunStaged(g4b_handle& h) {
     Check(cudaEventRecord(h.kernelTimer.start, h.stream), "cudaEventRecord");
     if (Form(h) == g4b::kBatched) {
         const unsigned grid{BatchedGrid(h)};
+        if (UsesGenerationPass(h)) {
+            SizeWaves(h);
+        }
         if (h.chunkAdaptive) {
             // at least eight queue grabs per warp, so that a small batch's
             // photons (and its tail) are shared out over every warp; never
@@ -1744,10 +1792,14 @@ int g4b_destroy(g4b_handle* handle) {
             cudaStreamSynchronize(stream);
         }
     }
-    std::vector<cudaEvent_t> events{handle->zeroedEvent, handle->orderedEvent[0], handle->orderedEvent[1]};
+    if (handle->orderStream != nullptr) {
+        cudaStreamSynchronize(handle->orderStream);
+    }
+    std::vector<cudaEvent_t> events{handle->zeroedEvent, handle->orderJoinEvent};
     for (std::uint32_t k{}; k < kWaveSlots; ++k) {
         events.push_back(handle->generatedEvent[k]);
         events.push_back(handle->storeFreeEvent[k]);
+        events.push_back(handle->parkedEvent[k]);
     }
     for (cudaEvent_t event : handle->joinEvents) {
         events.push_back(event);
@@ -1771,6 +1823,9 @@ int g4b_destroy(g4b_handle* handle) {
     }
     if (handle->generationStream != nullptr) {
         cudaStreamDestroy(handle->generationStream);
+    }
+    if (handle->orderStream != nullptr) {
+        cudaStreamDestroy(handle->orderStream);
     }
     if (handle->stream != nullptr) {
         cudaStreamDestroy(handle->stream);

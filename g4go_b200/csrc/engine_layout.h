@@ -185,7 +185,8 @@ struct PhotonStore {
     std::uint32_t* eventIndex;
 };
 constexpr std::uint32_t kPhotonStoreBytes{10U * 4U + 8U + 4U * 4U};  // per photon: 64
-constexpr std::uint32_t kPhotonStoreWave{1U << 26};                  // most photons in one generation wave
+constexpr std::uint32_t kPhotonStoreWave{1U << 28};                  // most photons in one generation wave
+constexpr std::uint32_t kPhotonStoreWaveMin{1U << 26};               // smallest wave the memory sizing picks
 constexpr std::uint32_t kWaveSlots{4};                                // generation-pass waves in flight at once
 
 // A photon of the generation pass's transport parked in the wave's queue,
@@ -219,7 +220,7 @@ struct DeferredQueue {
     std::uint32_t reserved;
 };
 constexpr std::uint32_t kDeferBounces{256};
-constexpr std::uint32_t kDeferredCapacity{1U << 19};  // per wave in flight (38 MB each)
+constexpr std::uint32_t kDeferredMinCapacity{1U << 19};  // per wave in flight (38 MB), or wave / 64 if more
 
 struct LaunchParams {
     const float4* emissions;               // [emissionCount] 128-byte gensteps as 8 float4 each

@@ -703,15 +703,11 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
                                              &job, parkOpen);
             }
         }
-        if constexpr (kPregenerated) {
-            if (alive && result == kLeftVolume) {
-                // untouched by the step: handed over whole, or (queue full)
-                // stepped again next iteration, now in place
-                if (DeferPhoton(p.deferred, photon)) {
-                    alive = false;
-                } else {
-                    parkOpen = false;
-                }
+        // a photon that left its volume is untouched by the step: parked below
+        bool leftVolume{false};
+        if constexpr (kPregenerated && !kParked) {
+            leftVolume = alive && result == kLeftVolume;
+            if (leftVolume) {
                 result = kContinue;
             }
         }
@@ -761,10 +757,12 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
                 alive = false;
             }
         }
-        if constexpr (kPregenerated) {
-            // a long history goes to the wave's queue launch, and the lane
-            // takes fresh work (identical results: the step is the same)
-            if (alive && photon.bounce >= kDeferBounces && parkOpen) {
+        if constexpr (kPregenerated && !kParked) {
+            // a photon that left its volume or whose history grew long goes
+            // to the wave's queue launch, and the lane takes fresh work
+            // (identical results: the step is the same); with the queue full
+            // it stays, and steps in place from now on
+            if (alive && (leftVolume || photon.bounce >= kDeferBounces) && parkOpen) {
                 if (DeferPhoton(p.deferred, photon)) {
                     alive = false;
                 } else {

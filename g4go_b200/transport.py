@@ -261,7 +261,7 @@ class PhotonTransportConfig:
     # batched FP32: 0/1 separate generation kernel for batches of >= 2^24 photons,
     # 2 generation inside the loop, 3 separate generation kernel at any size
     generation_pass: int = 0
-    wave_photons: int = 0  # most photons per generation-pass wave (0: 2^26)
+    wave_photons: int = 0  # most photons per generation-pass wave (0: sized by free device memory, <= 2^28)
     device: int = -1
 
     def to_c(self) -> _abi.Config:

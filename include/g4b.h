@@ -212,12 +212,15 @@ typedef struct g4b_config {
     uint32_t record_photon_fates;    /* 1 -> keep a per-photon fate/bounce/time record (diagnostics) */
     uint32_t generation_pass;        /* batched FP32 form: 0 or 1 -> the photons of a batch of at least 2^24
                                         photons are made by a separate generation kernel into a photon
-                                        store, in waves of up to 2^26 photons, and read by the transport
+                                        store, in waves of up to 2^28 photons, and read by the transport
                                         kernel (smaller batches generate inside the transport loop);
                                         2 -> always inside the transport loop;
                                         3 -> always the separate generation kernel, whatever the size */
     uint32_t wave_photons;           /* most photons in one generation-pass wave, rounded up to a multiple of
-                                        32; 0 -> 2^26. Smaller waves give a small batch several waves. */
+                                        32 (at most 2^28); 0 -> the largest of 2^28, 2^27, 2^26 whose photon
+                                        stores (64 B per photon, one per wave in flight, up to four) fit in
+                                        half of the free device memory, else 2^26. Smaller waves give a
+                                        small batch several waves. */
     uint32_t reserved[5];
 } g4b_config;
 

@@ -1,8 +1,8 @@
 """The batched FP32 form's generation pass against generation inside the loop.
 
 A batch of at least 2^24 photons has its photons made by GeneratePhotons into
-photon stores, in equal waves of at most 2^26 photons (two here), overlapped
-on a second stream, and captured into one CUDA graph or launched directly;
+photon stores, in equal waves (here of at most 2^26 photons: two), overlapped
+on streams of their own, and captured into one CUDA graph or launched directly;
 `generation_pass = 2` makes them inside the transport loop instead, the form
 the parity tests hold byte-exact against the oracle. Every photon comes from
 its own genstep and RNG counters either way, so the detections (in the
@@ -21,7 +21,7 @@ pytestmark = pytest.mark.gpu
 @pytest.fixture(scope="module")
 def large_batch():
     batch = scenes.workload("batched", event_count=3300, seed=11)
-    assert batch.photon_count > 2 ** 26  # two waves
+    assert batch.photon_count > 2 ** 26  # two waves of at most 2^26
     return scenes.crystal_sipm_scene(), batch
 
 
@@ -60,7 +60,7 @@ def test_generation_pass_matches_generation_in_the_loop(large_batch, graph, pinn
     try:
         inline, _ = run(scene, batch, generation_pass=2, use_cuda_graph=graph, ordered_detections=ordered)
         passed, replayed = run(scene, batch, pinned=buffer.array if pinned else None, generation_pass=0,
-                               use_cuda_graph=graph, ordered_detections=ordered)
+                               wave_photons=1 << 26, use_cuda_graph=graph, ordered_detections=ordered)
     finally:
         if buffer is not None:
             buffer.free()

@@ -8,8 +8,9 @@ ordered by MarkWaveSlots / ScatterWaveDetections. `generation_pass = 3` takes
 that path for a batch of any size, and `wave_photons` cuts a small batch into
 many waves, so the whole parity matrix runs through the benchmarked kernels at
 sizes the oracle finishes in seconds. The last test runs the default
-configuration on a real two-wave batch (more than 2^26 photons) and compares
-slices of whole events with the oracle run on the same photon slots.
+configuration on a real multi-wave batch (more than 2^28 photons, the largest
+wave) and compares slices of whole events with the oracle run on the same
+photon slots.
 """
 import functools
 
@@ -156,14 +157,16 @@ def event_slot_starts(batch):
 
 
 def test_default_configuration_two_wave_batch_matches_oracle_on_event_slices(oracle):
-    """The benchmark's own configuration on more than 2^26 photons: two waves,
-    generation pass, captured graph, ordered detections. The oracle transports
-    three slices of whole events (the first events, the events around the
-    boundary between the waves, the last events) on the same photon slots; the
-    engine's detections and counters for those events must be the oracle's."""
+    """The benchmark's own configuration on more than 2^28 photons: two waves
+    (or more, where the free device memory sizes them smaller), generation
+    pass, captured graph, ordered detections. The oracle transports three
+    slices of whole events (the first events, the events around the middle of
+    the batch, where two waves meet, the last events) on the same photon slots;
+    the engine's detections and counters for those events must be the
+    oracle's."""
     scene = scenes.crystal_sipm_scene()
-    batch = scenes.workload("batched", event_count=3300, seed=11)
-    assert batch.photon_count > 2 ** 26
+    batch = scenes.workload("batched", event_count=13000, seed=11)
+    assert batch.photon_count > 2 ** 28
     config = PhotonTransportConfig(seed=SEED)
     with TransportHost(config) as host:
         host.enqueue_emissions(scene, batch)
