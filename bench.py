@@ -64,7 +64,7 @@ def scheduler_leg(scene, events: int, local: int, producers: int = 8, window: in
     (include/g4b_scheduler.h) by `producers` native threads
     (g4b_scheduler_replay), each keeping at most `window` results
     outstanding (the reference's maxPendingEvents per worker,
-    PhotonTransportConfig.hpp:36): pipelined (two batches in flight) and in the reference's
+    PhotonTransportConfig.hpp:36): pipelined (eight batches in flight) and in the reference's
     serial order, both at the reference's batch target. Host wall clock from the first submission to the last result:
     the median of three passes after one warm-up pass, with the spread."""
     from g4go_b200 import PhotonTransportConfig, scenes

@@ -213,14 +213,20 @@ struct g4b_scheduler {
 
 namespace {
 
+// Most batches on the GPU at once (engine handles of a pipelined scheduler).
+// With the reference's closest-hit semantics a 1e6-photon batch ends in its
+// longest histories, serial chains of thousands of steps, so batches in
+// flight overlap one another's tails.
+constexpr std::uint32_t kMaxBatchesInFlight{8U};
+
 void ApplyDefaults(g4b_scheduler_config& c) {
     if (c.target_photons_per_batch == 0U) c.target_photons_per_batch = 1000000U;
     if (c.max_events_per_batch == 0U) c.max_events_per_batch = 10000U;
     if (c.max_queued_photons == 0U) c.max_queued_photons = 2000000U;
     if (c.max_queued_submissions == 0U) c.max_queued_submissions = 1024U;
     if (c.batch_collection_timeout_ms == 0U) c.batch_collection_timeout_ms = 10U;
-    if (c.batches_in_flight == 0U) c.batches_in_flight = 2U;
-    c.batches_in_flight = std::min(c.batches_in_flight, 4U);
+    if (c.batches_in_flight == 0U) c.batches_in_flight = kMaxBatchesInFlight;
+    c.batches_in_flight = std::min(c.batches_in_flight, kMaxBatchesInFlight);
 }
 
 template<class F>
@@ -717,8 +723,8 @@ int g4b_scheduler_create_with_transport(const g4b_transport_ops* ops, uint32_t o
         tLastError = "ABI version mismatch";
         return G4B_ERR_INVALID_ARGUMENT;
     }
-    if (opsCount < 1U || opsCount > 4U) {
-        tLastError = "a scheduler takes one to four transports";
+    if (opsCount < 1U || opsCount > kMaxBatchesInFlight) {
+        tLastError = "a scheduler takes one to eight transports";
         return G4B_ERR_INVALID_ARGUMENT;
     }
     for (uint32_t i{}; i < opsCount; ++i) {

@@ -703,6 +703,16 @@ __global__ void __launch_bounds__(256, BatchedMinBlocks<R>::value) TransportBatc
                                              &job, parkOpen);
             }
         }
+        if (result == kFresnelPendingLost) {
+            if constexpr (kRing >= 2U * 32U - 1U) {
+                result = kFresnelPending;  // the pass form parks such photons before they get here
+            } else {
+                // a photon that left its volume the way the reference lets it
+                // often reflects totally at every step for thousands of steps:
+                // in the ring it would advance one step per completion of 32
+                result = FinishFresnelHere(photon, job, p.seed, p.maxBounce, epsilon);
+            }
+        }
         // a photon that left its volume is untouched by the step: parked below
         bool leftVolume{false};
         if constexpr (kPregenerated && !kParked) {

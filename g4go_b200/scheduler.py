@@ -3,8 +3,8 @@
 Mirrors include/g4go/optical/geant4/OpticalBatchScheduler.hpp:32-93: producer
 threads submit one event's gensteps at a time and get a future for that
 event's detections and statistics; the native scheduler's transport thread
-batches the submissions and keeps two batches in flight on two engine
-handles. The ctypes calls release the GIL, so Python producer threads run
+batches the submissions and keeps up to batches_in_flight batches (eight by
+default) on the GPU, one per engine handle. The ctypes calls release the GIL, so Python producer threads run
 concurrently with one another and with the transport thread.
 """
 from __future__ import annotations
@@ -41,7 +41,7 @@ class BatchSchedulerConfig:
     batch_collection_timeout_ms: int = 10
     enable_performance_diagnostics: bool = False
     serial: bool = False  # the reference's order: retire a batch before collecting the next
-    batches_in_flight: int = 2  # pipelined: engine handles and batches on the GPU at once (at most 4)
+    batches_in_flight: int = 8  # pipelined: engine handles and batches on the GPU at once (at most 8)
 
     def to_c(self) -> _abi.SchedulerConfig:
         config = _abi.SchedulerConfig()
@@ -138,7 +138,7 @@ class OpticalBatchScheduler:
 
     transports: objects with enqueue(emissions, event_ids, emission_event_indices),
     poll() -> bool, query() -> (detections, events) and complete(output) driven
-    instead of engine handles (one to four; see g4b_scheduler_create_with_transport)."""
+    instead of engine handles (one to eight; see g4b_scheduler_create_with_transport)."""
 
     def __init__(self, config: PhotonTransportConfig | None = None, scene: Scene | None = None,
                  batching: BatchSchedulerConfig | None = None, transports: Sequence | None = None) -> None:

@@ -25,14 +25,14 @@ using TransportFuture = std::shared_future<TransportOutput>;
 
 class BatchScheduler final {
 public:
-    // Scheduler over the engine: two (or batches_in_flight) handles made
+    // Scheduler over the engine: batches_in_flight (0: eight) handles made
     // from `engine` with `scene` set on each.
     BatchScheduler(const g4b_config& engine, const g4b_scene& scene, const g4b_scheduler_config& batching)
         : fEngine{engine}, fScene{&scene}, fBatching{batching} {
         fEngine.abi_version = G4B_ABI_VERSION;
         fBatching.abi_version = G4B_ABI_VERSION;
     }
-    // Scheduler over caller-supplied transports (one to four).
+    // Scheduler over caller-supplied transports (one to eight).
     BatchScheduler(const std::vector<g4b_transport_ops>& transports, const g4b_scheduler_config& batching)
         : fTransports{transports}, fBatching{batching} {
         fBatching.abi_version = G4B_ABI_VERSION;

@@ -56,7 +56,7 @@ typedef struct g4b_scheduler_config {
     uint32_t batch_collection_timeout_ms;  /* 0 -> 10 */
     uint32_t enable_performance_diagnostics; /* 1: time queue waits and flattening, as the reference does */
     uint32_t serial;                       /* 1: the reference's order (retire batch k before collecting k+1); 0: pipelined */
-    uint32_t batches_in_flight;            /* pipelined: engine handles, and batches on the GPU at once; 0 -> 2, at most 4 */
+    uint32_t batches_in_flight;            /* pipelined: engine handles, and batches on the GPU at once; 0 -> 8, at most 8 */
     uint32_t reserved[7];
 } g4b_scheduler_config;
 
