@@ -177,3 +177,37 @@ def test_caller_detection_buffers_are_checked_before_the_engine_writes():
                 readonly, np.empty((2, 4), dtype=transport.DETECTION_DTYPE)):
         with pytest.raises(ValueError):
             host.complete_oldest_batch(detections_out=bad)
+
+
+# the ctypes view of every record the C ABI passes, and the C struct it mirrors
+CTYPES_RECORDS = {
+    "Config": "g4b_config", "Property": "g4b_property", "Material": "g4b_material", "Surface": "g4b_surface",
+    "Volume": "g4b_volume", "SurfaceBinding": "g4b_surface_binding", "Scene": "g4b_scene",
+    "Statistics": "g4b_statistics", "EventStatistics": "g4b_event_statistics", "Performance": "g4b_performance",
+    "Output": "g4b_output", "TuneResult": "g4b_tune_result", "GradientRequest": "g4b_gradient_request",
+    "Gradients": "g4b_gradient_result", "SchedulerConfig": "g4b_scheduler_config",
+    "BatchStatistics": "g4b_batch_statistics", "TransportOps": "g4b_transport_ops", "SynthParams": "g4b_synth_params",
+}
+
+
+def test_every_ctypes_field_sits_where_the_header_puts_it(tmp_path):
+    """Size and the offset of every field of each ctypes record, from a C
+    compiler on include/*.h, so that a field added to a header without its
+    ctypes mirror (or the other way round) fails here, not on a GPU."""
+    from g4go_b200 import _abi
+
+    checks = []
+    for py_name, c_name in CTYPES_RECORDS.items():
+        record = getattr(_abi, py_name)
+        checks.append((f"sizeof({c_name})", C.sizeof(record), py_name))
+        for field in record._fields_:
+            checks.append((f"offsetof({c_name}, {field[0]})", getattr(record, field[0]).offset, f"{py_name}.{field[0]}"))
+    program = tmp_path / "fields.c"
+    body = "".join(f' printf("%zu\\n", (size_t){expr});\n' for expr, _, _ in checks)
+    program.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "g4b.h"\n#include "g4b_synth.h"\n'
+                       '#include "g4b_scheduler.h"\nint main(void){\n' + body + " return 0; }\n")
+    exe = tmp_path / "fields"
+    subprocess.run(["gcc", "-std=c11", "-I", str(ROOT / "include"), str(program), "-o", str(exe)], check=True)
+    values = list(map(int, subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()))
+    mismatches = [(what, c, py) for (_, py, what), c in zip(checks, values) if c != py]
+    assert not mismatches, mismatches
