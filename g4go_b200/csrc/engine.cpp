@@ -1021,11 +1021,11 @@ std::uint64_t LaunchBatchedWaves(g4b_handle& h, const LaunchParams& base, unsign
     return launches;
 }
 
-// The generation-pass waves as a CUDA graph: captured from the two streams
-// on every run (the launch parameters and wave count follow the batch),
-// applied to the previous executable graph when its shape still fits and
-// instantiated afresh when it does not, then launched. Relaunches of a batch
-// therefore replay one graph of 2 + 3 x waves nodes.
+// The generation-pass waves as a CUDA graph: captured from the handle's
+// streams (transport, generation, ordering) on every run (the launch
+// parameters and wave count follow the batch), applied to the previous
+// executable graph when its shape still fits and instantiated afresh when it
+// does not, then launched. Relaunches of a batch therefore replay one graph.
 std::uint64_t LaunchBatchedWavesGraph(g4b_handle& h, const LaunchParams& base, unsigned grid, std::uint32_t block) {
     PrepareWaves(h);  // allocations stay outside the capture
     Check(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
